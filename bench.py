@@ -1,0 +1,312 @@
+"""Benchmark: grid-point RK4 updates per second on the stratified-shell workload.
+
+Workload (N = 1): 6 x 128^3 stratified spherical shell (r in [0.7, 1]; c = 0.1 + 0.9 s^0.5,
+rho0 = (s + 0.01)^1.5, s = (1-r)/0.3; outer-5% sponge; one Gaussian pulse).  A "step" is
+one call of the reference's RK4 (timestep.f90:41-86): five 2N-storage stages (edge
+exchange + fused RHS/BC/sponge/update) and the explicit filter.  The unit of work is one
+grid point advanced one full step.
+
+* value       FP32 fused path (4 fields; rho is write-only with g0 = 0), device-resident,
+              CUDA events on the library stream, K steps after W warm-up steps.
+* fp64        the plain FP64 path (5 fields) on the same workload, for the FP32-vs-FP64
+              comparison; fp32_rel_err_vs_fp64 is the per-field relative L2 after the run.
+* e2e         the same metric through the C-ABI with host buffers: state uploaded from
+              pinned host memory, RK4 called once per step with the reference's per-step
+              norm (cube.f90:77) read back, final state downloaded.
+* roofline    the dominant kernel (the fused stage kernel): algorithmic bytes per launch
+              (q and qw read, q and qw written; 3F words in stage 1, 4F in stages 2-5)
+              over its mean launch time from per-launch CUDA events.
+* cpu_baseline the FP64 C++ restatement of the reference (the oracle), all host cores.
+
+N > 1: one process per GPU (torchrun), each GPU runs its own replica of the workload
+(weak scaling; the runs are independent, no collective on the data path); value is the
+total over ranks with the time taken as the max over ranks.
+``--impl reference`` times the reference's CPU path (the oracle port) instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        except Exception:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_baseline(cfg, nsteps: int):
+    import oracle
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    o = oracle.Oracle(cfg)
+    q = o.initial_state()
+    t0 = time.perf_counter()
+    q = o.rk4(q, nsteps)
+    dt = time.perf_counter() - t0
+    return {"value": cfg.points * nsteps / dt, "unit": "grid-pt RK4 updates/s", "cores": threads,
+            "kind": "port",
+            "sample": f"{nsteps} full RK4 step(s) of the 6x{cfg.nx}^3 workload, FP64 C++ restatement "
+                      f"of the reference (OpenMP, {threads} threads), {dt:.2f} s"}
+
+
+def run_reference(args, world, rank):
+    """The reference's CPU path (the oracle port) on the bench workload, rank 0 only."""
+    if rank != 0:
+        return
+    from solar_b200 import configs
+    import oracle
+    cfg = configs.get(args.config)
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    o = oracle.Oracle(cfg)
+    q = o.initial_state()
+    q = o.rk4(q, args.warmup)
+    t0 = time.perf_counter()
+    q = o.rk4(q, args.steps)
+    dt = time.perf_counter() - t0
+    value = cfg.points * args.steps / dt
+    line = {
+        "impl": "reference", "metric": "grid-pt RK4 updates/s", "value": value, "unit": "grid-pt RK4 updates/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": workload_name(cfg), "nx": cfg.nx, "nr": cfg.nr, "points": cfg.points},
+        "cpu_baseline": {"value": value, "unit": "grid-pt RK4 updates/s", "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} full RK4 steps after {args.warmup} warm-up, FP64 C++ restatement "
+                                   f"of the reference, OpenMP {threads} threads"},
+        "e2e": {"value": value, "unit": "grid-pt RK4 updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def workload_name(cfg):
+    return (f"{cfg.name}: 6 x {cfg.nx}^2 x {cfg.nr} stratified spherical shell, CFL 0.5 dt={cfg.dt:.4g}, "
+            f"sponge {cfg.sponge.length} outer points")
+
+
+def rel_errors(a, b, fields):
+    names = ("rho", "v_xi", "v_eta", "v_r", "p")
+    return {names[m]: float(np.linalg.norm(a[:, m] - b[:, m]) / max(np.linalg.norm(b[:, m]), 1e-300)) for m in fields}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="solar", choices=["solar", "reference"])
+    ap.add_argument("--config", default="c2")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+
+    from solar_b200 import configs
+    from solar_b200.solver import Solver
+
+    cfg = configs.get(args.config)
+    pts = cfg.points
+    peak, peak_kind = load_peaks()
+
+    # ---------------------------------------------------------------- FP32 fused path
+    s32 = Solver(cfg, precision="fp32", nfields=4, device=local)
+    s32.init_sources()
+    s32.rk4(args.warmup)
+    barrier(world)
+    s32.synchronize()
+    with ClockSampler(local) as clk:
+        t = s32.time_rk4(args.steps)
+    barrier(world)
+    ms32 = max_over_ranks(t["total_ms"], world)
+    value = pts * args.steps * world / (ms32 / 1e3)
+    q32 = s32.get_state()
+
+    # per-kernel launch times (graph off) for the roofline of the dominant kernel
+    kt = s32.time_rk4(max(4, min(args.steps, 20)), per_kernel=True)
+    F, w = 4, 4
+    stage_bytes = (3 * F + 4 * 4 * F) / 5.0 * w * pts          # mean algorithmic bytes per stage launch
+    filter_bytes = 2 * F * w * pts
+    stage_gbs = stage_bytes / (kt["stage_ms"] / 1e3) / 1e9
+    filter_gbs = filter_bytes / (kt["filter_ms"] / 1e3) / 1e9
+    step_bytes = 21 * F * w * pts
+    s32.close()
+
+    # ---------------------------------------------------------------- FP64 plain path
+    s64 = Solver(cfg, precision="fp64", nfields=5, device=local)
+    s64.init_sources()
+    s64.rk4(args.warmup)
+    barrier(world)
+    t64 = s64.time_rk4(args.steps)
+    barrier(world)
+    ms64 = max_over_ranks(t64["total_ms"], world)
+    value64 = pts * args.steps * world / (ms64 / 1e3)
+    q64 = s64.get_state()
+    kt64 = s64.time_rk4(4, per_kernel=True)
+    s64.close()
+    err = rel_errors(q32, q64, (1, 2, 3, 4))
+
+    # ---------------------------------------------------------------- end to end (C-ABI, host buffers)
+    e2e = None
+    if not args.no_e2e:
+        import torch
+        state_bytes = 6 * 5 * cfg.nr * cfg.nx * cfg.nx * 8
+        host = torch.empty(6 * 5 * cfg.nr * cfg.nx * cfg.nx, dtype=torch.float64, pin_memory=True).numpy()
+        out = torch.empty_like(torch.from_numpy(host)).pin_memory().numpy()
+        with Solver(cfg, precision="fp32", nfields=4, device=local) as se:
+            se.init_sources()
+            se.get_state(out=host.reshape(se.state_shape))
+            se.rk4(args.warmup)
+            barrier(world)
+            t0 = time.perf_counter()
+            se.set_state(host.reshape(se.state_shape))
+            norms = []
+            for _ in range(args.steps):
+                se.rk4(1)
+                norms.append(se.norm(4))
+            se.get_state(out=out.reshape(se.state_shape))
+            te = time.perf_counter() - t0
+        te = max_over_ranks(te, world)
+        e2e = {"value": pts * args.steps * world / te, "unit": "grid-pt RK4 updates/s",
+               "h2d_bytes_per_step": state_bytes / args.steps,
+               "d2h_bytes_per_step": state_bytes / args.steps + 8,
+               "note": "state in from pinned host memory once, RK4 + norm(v_r) read back every step "
+                       "(cube.f90:74-78), state out at the end; timed per job of K steps"}
+
+    if rank != 0:
+        return
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(cfg, 2)
+    clocks = clk.summary()
+    line = {
+        "metric": "grid-pt RK4 updates/s (FP32 fused path; FP64 plain path in fp64)",
+        "value": value, "unit": "grid-pt RK4 updates/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": workload_name(cfg), "nx": cfg.nx, "nr": cfg.nr, "points": pts,
+                   "parallelism": f"replica x{world}", "fields": 4,
+                   "l2": "inputs larger than L2: three state buffers of %.0f MB each" % (
+                       6 * 4 * cfg.nr * (cfg.nx + 6) * (cfg.nx + 16) * 4 / 1e6)},
+        "fp64": {"value": value64, "ms_per_step": ms64 / args.steps, "fields": 5,
+                 "fp32_speedup": value / value64,
+                 "stage_ms": kt64["stage_ms"], "filter_ms": kt64["filter_ms"], "edge_ms": kt64["edge_ms"]},
+        "fp32_rel_err_vs_fp64": err,
+        "roofline": {"bound": "hbm", "achieved": stage_gbs, "peak": peak, "unit": "GB/s",
+                     "frac": stage_gbs / peak, "traffic": None, "peak_kind": peak_kind,
+                     "kernel": "stage_kernel<float,32,8>", "algorithmic_bytes_per_launch": stage_bytes,
+                     "mean_launch_ms": kt["stage_ms"],
+                     "filter": {"achieved": filter_gbs, "frac": filter_gbs / peak, "mean_launch_ms": kt["filter_ms"]},
+                     "edge_mean_launch_ms": kt["edge_ms"],
+                     "step_roofline_pt_steps_per_s": peak * 1e9 / (21 * F * w),
+                     "step_frac": (value / world) * (21 * F * w) / (peak * 1e9)},
+        "gpu_launches": 12 * args.steps,
+        "clocks": clocks,
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

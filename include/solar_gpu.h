@@ -1,0 +1,152 @@
+/*
+ * solar_gpu.h -- C-ABI of the B200 (sm_100a) time-stepping engine for the cubed-sphere
+ * linear-acoustics solver ankitvb/solar.
+ *
+ * The reference is Fortran 90 + MPI.  Its time-stepping path is a link-time plug-in
+ * surface (makefile:14-18): external subroutines RK4 (timestep.f90:41), COMPUTE_RHS
+ * (compute_rhs_acoustic.f90:1), BC_RHS (bc_acoustic_wave.f90:1), SPONGE (sponge.f90:1)
+ * and the module procedure FILTER_EXP (filter.f90:9), all working on the state
+ * q(mx,my,mr,5) of COMMON /RKWORK/ (cube.f90:18-20).  This header is the C side of that
+ * surface for a host that drives all six cubed-sphere faces from one process: every
+ * entry point takes plain pointers and sizes, returns an int status and never aborts.
+ *
+ * Array layout of every host array below (FP64, "six-zone Fortran order"): the six
+ * per-zone Fortran arrays concatenated in zone order 1..6,
+ *    field arrays   f[zone][k][j][i]          = f(mx,my,mr) of each zone, i fastest
+ *    state arrays   q[zone][m][k][j][i]       = q(mx,my,mr,5) of each zone,
+ *                                               m = rho, v_xi, v_eta, v_r, p
+ * with mx = my = nx and mr = nr (the reference's px = py = pr = 1 case).  A Fortran
+ * host with one zone per rank passes its q(:,:,:,:) directly for one zone slot.
+ *
+ * Threading: a context belongs to one host thread and one CUDA device; calls are
+ * stream-ordered on the context's own stream and complete before they return.
+ */
+#ifndef SOLAR_GPU_H
+#define SOLAR_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SOLAR_GPU_ABI_VERSION 1
+
+/* Status codes.  SOLAR_ERR_* are negative; solar_gpu_last_error() has the detail. */
+#define SOLAR_OK 0
+#define SOLAR_ERR_ARG (-1)      /* bad argument or unsupported size                  */
+#define SOLAR_ERR_CUDA (-2)     /* a CUDA runtime call failed                        */
+#define SOLAR_ERR_NAN (-3)      /* the NaN/Inf watchdog tripped                      */
+#define SOLAR_ERR_TIMEOUT (-4)  /* a bounded device wait gave up                     */
+#define SOLAR_ERR_STATE (-5)    /* context not initialised / wrong call order        */
+#define SOLAR_ERR_NOMEM (-6)    /* device or pinned host allocation failed           */
+
+#define SOLAR_FP64 0            /* state, stencils and accumulation in double        */
+#define SOLAR_FP32 1            /* state and stencils in float; metric, interpolation
+                                   weights and diagnostics computed once in double   */
+
+typedef struct solar_ctx solar_ctx;
+
+/* Run configuration.  Everything the reference fixes at compile time in 'header'
+ * (header:4-10) or hard-codes in the plug-ins becomes a field here; the defaults from
+ * solar_desc_defaults() equal the reference's values. */
+typedef struct solar_desc {
+  int nx;          /* points per face edge, nx = ny (header:4); multiple of 16, >= 16      */
+  int nr;          /* radial points (header:4); >= 16                                      */
+  int precision;   /* SOLAR_FP64 | SOLAR_FP32                                               */
+  int nfields;     /* 5: the reference's (rho, v, p).  4: rho dropped -- only valid when
+                      g0 == 0, where rho is write-only (compute_rhs_acoustic.f90:83, 146)  */
+  int nruns;       /* independent runs held side by side (batched sources); >= 1          */
+  int device;      /* CUDA device ordinal                                                  */
+  double dt;       /* deltat; the reference overrides its CFL estimate (timestep.f90:35),
+                      so the host sets it                                                  */
+  const double* model;   /* nr x 8 'solar_model' rows, row-major (r/R, c, rho, p, T, g,
+                            Gamma, unused), normalised here as SOLAR_DATA does
+                            (ic_acoustic_wave.f90:236-271)                                  */
+  const double* c2_3d;   /* optional six-zone field of c^2 replacing the radial c^2 (a 3-D
+                            sound-speed perturbation); NULL = radial background            */
+  double sponge_amp;     /* a_sponge = 0.1   (sponge.f90:20)                               */
+  double sponge_exp;     /* s_exp = 3        (sponge.f90:21)                               */
+  int sponge_len;        /* k_sponge_length = 30 (sponge.f90:27)                           */
+  int sponge_lower;      /* keep the inner-end branch (sponge.f90:42-43); default 1        */
+  int sponge_upper;      /* keep the outer-end branch (sponge.f90:40-41); default 1        */
+  int fix_reversed_rotation; /* 0 (default) = reference arithmetic.  1 = evaluate the
+                            receiver-frame rotation of the eight reversed vector strips
+                            (transform.f90:184-274) at the receiver's mirrored edge index  */
+  int tile_x, tile_y, kchunk; /* stage-kernel tile; 0 = tuned default                     */
+} solar_desc;
+
+/* Fill *d with the reference's defaults (sizes 0, FP64, 5 fields, 1 run, device 0,
+ * sponge 0.1 / 3 / 30 at both ends). */
+void solar_desc_defaults(solar_desc* d);
+
+/* Setup sequence of cube.f90:35-51 (SOLAR_DATA, SETUP_COORDINATES_METRICS_ALL,
+ * SETUP_LAGRANGE_INTERPOLANT): builds the FP64 metric, background, interpolation and
+ * edge-rotation tables on the host, uploads them, and allocates the device state.  The
+ * state starts at zero (GENERATE_IC, ic_acoustic_wave.f90:4-29). */
+int solar_gpu_init(const solar_desc* d, solar_ctx** out);
+
+/* Release every device and host resource of the context. */
+int solar_gpu_finalize(solar_ctx* c);
+
+/* COMMON /RKWORK/ q (cube.f90:18-20): copy one run's state in / out, six-zone Fortran
+ * order, 6*5*nr*nx*nx doubles.  With nfields = 4 the rho slot reads back as 0. */
+int solar_gpu_set_state(solar_ctx* c, int run, const double* q);
+int solar_gpu_get_state(solar_ctx* c, int run, double* q);
+
+/* IC plug-in (GENERATE_IC slot, makefile:16): p += amp exp(-|x-x0|^2 / (2 width^2)) at
+ * the grid points x = r (unit vector of the zone's cube point). */
+int solar_gpu_add_gaussian(solar_ctx* c, int run, double x0, double y0, double z0,
+                           double width, double amp);
+
+/* RK4 (timestep.f90:41-86): nsteps calls of the reference's RK4 -- five 2N-storage
+ * stages of COMPUTE_RHS + BC_RHS + SPONGE + update, then FILTER_EXP -- on every run. */
+int solar_gpu_rk4(solar_ctx* c, int nsteps);
+
+/* Batched RK4: run r advances nsteps_per_run[r] steps (uneven counts), all runs in the
+ * same launches, replayed from one captured CUDA graph. */
+int solar_gpu_rk4_runs(solar_ctx* c, const int* nsteps_per_run);
+
+/* Operator-level drop-ins (host arrays in, host arrays out; use run 0's buffers):
+ *   COMPUTE_RHS (compute_rhs_acoustic.f90:1-159, forcing off)        q -> rhs
+ *   BC_RHS      (bc_acoustic_wave.f90:1-36)                          rhs in place
+ *   SPONGE      (sponge.f90:1-58)                                    q, rhs in place
+ *   FILTER_EXP  (filter.f90:9-48)                                    q -> qf
+ *   COMPUTE_GRADIENT  (grad.f90:13-59)     field p -> (grad_xi, grad_eta, grad_r)
+ *   COMPUTE_DIVERGENCE (grad.f90:62-136)   fields (v_xi, v_eta, v_r) -> div        */
+int solar_gpu_compute_rhs(solar_ctx* c, const double* q, double* rhs);
+int solar_gpu_bc_rhs(solar_ctx* c, double* rhs);
+int solar_gpu_sponge(solar_ctx* c, const double* q, double* rhs);
+int solar_gpu_filter_exp(solar_ctx* c, const double* q, double* qf);
+int solar_gpu_gradient(solar_ctx* c, const double* p, double* grad_xi, double* grad_eta,
+                       double* grad_r);
+int solar_gpu_divergence(solar_ctx* c, const double* v_xi, const double* v_eta,
+                         const double* v_r, double* div);
+
+/* norm (auxiliary.f90:100-125) of field m (1..5) of one run, in double:
+ * (sum(f^2) / (nx*ny*nr) * 6)^0.5 over the six zones, the reference's formula. */
+int solar_gpu_norm(solar_ctx* c, int run, int field, double* out);
+
+/* FP64 diagnostics of one run: out[0] = acoustic energy
+ * 1/2 sum (rho0 |v|^2 + p^2 / (rho0 c^2)) dV, out[1] = sum rho dV, out[2] = max |p|,
+ * out[3] = 1 if any value is NaN/Inf.  dV is the cubed-sphere volume element
+ * r^2 (1+X^2)(1+Y^2) / delta^(3/2) dxi deta dr. */
+int solar_gpu_diag(solar_ctx* c, int run, double* out4);
+
+/* Timed helpers for benchmarks: run nsteps of solar_gpu_rk4 with CUDA events on the
+ * context's stream.  out[0] = total ms; with per_kernel != 0 the steps are launched
+ * without the CUDA graph and out[1..3] = mean ms per launch of the stage, filter and
+ * edge kernels, out[4..6] = launches of each kind. */
+int solar_gpu_time_rk4(solar_ctx* c, int nsteps, int per_kernel, double* out7);
+
+/* Block until the context's stream is idle. */
+int solar_gpu_synchronize(solar_ctx* c);
+
+/* Copy the last error message of this thread (NUL-terminated, truncated to len). */
+int solar_gpu_last_error(char* buf, int len);
+
+/* ABI version (SOLAR_GPU_ABI_VERSION). */
+int solar_gpu_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SOLAR_GPU_H */

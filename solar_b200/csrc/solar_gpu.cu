@@ -1,0 +1,694 @@
+// solar_gpu.cu -- context management and the C-ABI of include/solar_gpu.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/solar_gpu.h"
+#include "kernels.cuh"
+#include "tables.h"
+
+namespace solar {
+
+thread_local std::string g_last_error;
+
+static int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+#define CK(call)                                                                          \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      return fail(SOLAR_ERR_CUDA, "%s:%d %s: %s", __FILE__, __LINE__, #call,              \
+                  cudaGetErrorString(e_));                                                \
+  } while (0)
+
+struct DevTables {
+  void* rad = nullptr;     // T [kNumRadial][nr]
+  void* met = nullptr;     // T [kNumMetric][n][n]
+  void* conv = nullptr;    // T [3][4][n][n]
+  void* w9 = nullptr;      // T [3][n][9]
+  void* rot = nullptr;     // T [6][4][3][n][2]
+  void* c2 = nullptr;      // T [6][nr][n][n] optional
+  int* s0 = nullptr;       // [3][n]
+  double* rad64 = nullptr; // FP64 copies for diagnostics
+  double* vol2 = nullptr;  // [n][n]
+  double* drw = nullptr;   // [nr]
+  double* c2_64 = nullptr; // optional
+  double* tanx = nullptr;  // [n]
+  double* gr = nullptr;    // [nr]
+};
+
+}  // namespace solar
+
+using namespace solar;
+
+struct solar_ctx {
+  solar_desc desc;
+  HostTables ht;
+  Geom g;
+  int fp32 = 0;
+  size_t esize = 8;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  void* A = nullptr;       // state
+  void* B = nullptr;       // stage ping-pong
+  void* W = nullptr;       // RK register qw
+  double* stage64 = nullptr;   // one (face, field) compact FP64 volume
+  double* part = nullptr;      // reduction partials
+  double* red_out = nullptr;   // reduction result (device)
+  int* active = nullptr;       // batched runs
+  int* target = nullptr;
+  int* done = nullptr;
+  DevTables dt;
+  int tile_x = 32, tile_y = 8, kchunk = 0;
+  cudaGraphExec_t step_graph = nullptr;
+  cudaGraphExec_t batch_graph = nullptr;
+  cudaEvent_t ev[8] = {};
+};
+
+namespace solar {
+
+template <typename T>
+static int upload(void** dst, const std::vector<double>& src) {
+  std::vector<T> tmp(src.begin(), src.end());
+  CK(cudaMalloc(dst, tmp.size() * sizeof(T)));
+  CK(cudaMemcpy(*dst, tmp.data(), tmp.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return SOLAR_OK;
+}
+
+template <typename T>
+static int upload_tables(solar_ctx* c) {
+  int rc;
+  if ((rc = upload<T>(&c->dt.rad, c->ht.radial))) return rc;
+  if ((rc = upload<T>(&c->dt.met, c->ht.metric))) return rc;
+  if ((rc = upload<T>(&c->dt.conv, c->ht.conv))) return rc;
+  if ((rc = upload<T>(&c->dt.w9, c->ht.w9))) return rc;
+  if ((rc = upload<T>(&c->dt.rot, c->ht.rot))) return rc;
+  return SOLAR_OK;
+}
+
+static int upload_constants() {
+  double drp[4], bdy[3][7], filt[4], filtr[6];
+  float drpf[4], bdyf[3][7], filtf[4], filtrf[6];
+  for (int m = 0; m < 4; ++m) { drp[m] = kDrp[m]; drpf[m] = (float)kDrp[m]; }
+  for (int r = 0; r < 3; ++r)
+    for (int m = 0; m < 7; ++m) { bdy[r][m] = kBdy[r][m]; bdyf[r][m] = (float)kBdy[r][m]; }
+  for (int m = 0; m < 4; ++m) { filt[m] = kFilt[m]; filtf[m] = (float)kFilt[m]; }
+  for (int m = 0; m < 6; ++m) { filtr[m] = kFiltR[m]; filtrf[m] = (float)kFiltR[m]; }
+  EdgeRouteDev rt[6][4];
+  for (int f = 0; f < 6; ++f)
+    for (int e = 0; e < 4; ++e) rt[f][e] = {kRoutes[f][e].src_face, kRoutes[f][e].src_edge, kRoutes[f][e].reversed};
+  CK(cudaMemcpyToSymbol(cDrpD, drp, sizeof(drp)));
+  CK(cudaMemcpyToSymbol(cBdyD, bdy, sizeof(bdy)));
+  CK(cudaMemcpyToSymbol(cFiltD, filt, sizeof(filt)));
+  CK(cudaMemcpyToSymbol(cFiltRD, filtr, sizeof(filtr)));
+  CK(cudaMemcpyToSymbol(cDrpF, drpf, sizeof(drpf)));
+  CK(cudaMemcpyToSymbol(cBdyF, bdyf, sizeof(bdyf)));
+  CK(cudaMemcpyToSymbol(cFiltF, filtf, sizeof(filtf)));
+  CK(cudaMemcpyToSymbol(cFiltRF, filtrf, sizeof(filtrf)));
+  CK(cudaMemcpyToSymbol(cRoute, rt, sizeof(rt)));
+  return SOLAR_OK;
+}
+
+// ---------------------------------------------------------------- launches
+template <typename T>
+static void launch_edge(solar_ctx* c, void* buf, int mode, const int* active) {
+  EdgeArgs<T> a;
+  a.q = (T*)buf;
+  a.w9 = (const T*)c->dt.w9;
+  a.s0 = c->dt.s0;
+  a.conv = (const T*)c->dt.conv;
+  a.rot = (const T*)c->dt.rot;
+  a.active = active;
+  a.g = c->g;
+  a.mode = mode;
+  dim3 block(64, 3);
+  dim3 grid((c->g.n + 63) / 64, c->g.nr, c->g.nruns * 24);
+  edge_kernel<T><<<grid, block, 0, c->stream>>>(a);
+}
+
+template <typename T, int TX, int TY>
+static void launch_stage_t(solar_ctx* c, const StageArgs<T>& a, int mode) {
+  const int nchunks = (c->g.nr + a.kchunk - 1) / a.kchunk;
+  dim3 grid((c->g.n / TX) * (c->g.n / TY), nchunks, c->g.nruns * 6);
+  dim3 block(TX, TY);
+  switch (mode) {
+    case 0: stage_kernel<T, TX, TY, 0><<<grid, block, 0, c->stream>>>(a); break;
+    case 1: stage_kernel<T, TX, TY, 1><<<grid, block, 0, c->stream>>>(a); break;
+    case 2: stage_kernel<T, TX, TY, 2><<<grid, block, 0, c->stream>>>(a); break;
+    default: stage_kernel<T, TX, TY, 3><<<grid, block, 0, c->stream>>>(a); break;
+  }
+}
+
+template <typename T>
+static void launch_stage(solar_ctx* c, const void* qin, void* qout, int mode, int stage,
+                         const int* active) {
+  StageArgs<T> a;
+  a.qin = (const T*)qin;
+  a.qout = (T*)qout;
+  a.qw = (T*)c->W;
+  a.rad = (const T*)c->dt.rad;
+  a.met = (const T*)c->dt.met;
+  a.c2 = (const T*)c->dt.c2;
+  a.active = active;
+  a.g = c->g;
+  a.dt = (T)c->desc.dt;
+  a.alpha = (T)kAlpha[stage];
+  a.beta = (T)kBeta[stage];
+  a.inv_dxi = (T)(1.0 / c->ht.dxi);
+  a.kchunk = c->kchunk;
+  if (c->tile_x == 16 && c->tile_y == 8) launch_stage_t<T, 16, 8>(c, a, mode);
+  else if (c->tile_x == 32 && c->tile_y == 4) launch_stage_t<T, 32, 4>(c, a, mode);
+  else if (c->tile_x == 32 && c->tile_y == 16) launch_stage_t<T, 32, 16>(c, a, mode);
+  else if (c->tile_x == 16 && c->tile_y == 16) launch_stage_t<T, 16, 16>(c, a, mode);
+  else launch_stage_t<T, 32, 8>(c, a, mode);
+}
+
+template <typename T>
+static void launch_filter(solar_ctx* c, const void* qin, void* qout, const int* active) {
+  FilterArgs<T> a;
+  a.qin = (const T*)qin;
+  a.qout = (T*)qout;
+  a.active = active;
+  a.g = c->g;
+  if (c->g.n % 32 == 0) {
+    dim3 grid((c->g.n / 32) * (c->g.n / 8), c->g.nf, c->g.nruns * 6);
+    filter_kernel<T, 32, 8><<<grid, dim3(32, 8), 0, c->stream>>>(a);
+  } else {
+    dim3 grid((c->g.n / 16) * (c->g.n / 8), c->g.nf, c->g.nruns * 6);
+    filter_kernel<T, 16, 8><<<grid, dim3(16, 8), 0, c->stream>>>(a);
+  }
+}
+
+// One full time step (timestep.f90:61-82) on every run.  With ev != nullptr each kernel
+// is bracketed by events: ev_pairs[kind] accumulates into times[kind].
+template <typename T>
+static void enqueue_step(solar_ctx* c, const int* active, std::vector<cudaEvent_t>* evs) {
+  void* bufs[2] = {c->A, c->B};
+  int cur = 0;
+  auto mark = [&]() {
+    if (!evs) return;
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    cudaEventRecord(e, c->stream);
+    evs->push_back(e);
+  };
+  for (int s = 0; s < 5; ++s) {
+    mark();
+    launch_edge<T>(c, bufs[cur], 0, active);
+    mark();
+    launch_stage<T>(c, bufs[cur], bufs[cur ^ 1], s == 0 ? 1 : 0, s, active);
+    mark();
+    cur ^= 1;
+  }
+  mark();
+  launch_edge<T>(c, bufs[cur], 1, active);
+  mark();
+  launch_filter<T>(c, bufs[cur], bufs[cur ^ 1], active);
+  mark();
+}
+
+static void enqueue_step_any(solar_ctx* c, const int* active, std::vector<cudaEvent_t>* evs) {
+  if (c->fp32) enqueue_step<float>(c, active, evs);
+  else enqueue_step<double>(c, active, evs);
+}
+
+static int capture_step_graph(solar_ctx* c) {
+  if (c->step_graph) return SOLAR_OK;
+  cudaGraph_t graph;
+  CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  enqueue_step_any(c, nullptr, nullptr);
+  CK(cudaStreamEndCapture(c->stream, &graph));
+  CK(cudaGraphInstantiate(&c->step_graph, graph, 0));
+  CK(cudaGraphDestroy(graph));
+  return SOLAR_OK;
+}
+
+static int capture_batch_graph(solar_ctx* c) {
+  if (c->batch_graph) return SOLAR_OK;
+  const int R = c->g.nruns;
+  cudaGraph_t graph;
+  CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  batch_tick_kernel<<<(R + 127) / 128, 128, 0, c->stream>>>(c->target, c->done, c->active, R);
+  enqueue_step_any(c, c->active, nullptr);
+  batch_tock_kernel<<<(R + 127) / 128, 128, 0, c->stream>>>(c->active, c->done, R);
+  CK(cudaStreamEndCapture(c->stream, &graph));
+  CK(cudaGraphInstantiate(&c->batch_graph, graph, 0));
+  CK(cudaGraphDestroy(graph));
+  return SOLAR_OK;
+}
+
+// ---------------------------------------------------------------- transfers
+static long long vol_compact(const solar_ctx* c) { return (long long)c->g.n * c->g.n * c->g.nr; }
+
+// Host six-zone field(s) -> device padded slot volumes of `buf`, for run `run`.
+// `fields` lists the reference fields present in the host array in order; the host array
+// holds nh fields per zone (5 for a state, 1 for a single field).
+static int upload_fields(solar_ctx* c, void* buf, int run, const double* host, int nh,
+                         const int* fields, int nfields_h) {
+  const long long V = vol_compact(c);
+  const int threads = 256;
+  const int blocks = (int)((V + threads - 1) / threads);
+  for (int z = 0; z < 6; ++z)
+    for (int m = 0; m < nfields_h; ++m) {
+      const int f = fields[m];
+      const int s = c->g.slot[f];
+      if (s < 0) continue;
+      CK(cudaMemcpyAsync(c->stage64, host + ((long long)z * nh + m) * V, V * sizeof(double),
+                         cudaMemcpyHostToDevice, c->stream));
+      const long long off = c->g.vol(run, z, s);
+      if (c->fp32) unpack_kernel<float><<<blocks, threads, 0, c->stream>>>(c->stage64, (float*)buf + off, c->g);
+      else unpack_kernel<double><<<blocks, threads, 0, c->stream>>>(c->stage64, (double*)buf + off, c->g);
+      CK(cudaGetLastError());
+    }
+  return SOLAR_OK;
+}
+
+static int download_fields(solar_ctx* c, const void* buf, int run, double* host, int nh,
+                           const int* fields, int nfields_h) {
+  const long long V = vol_compact(c);
+  const int threads = 256;
+  const int blocks = (int)((V + threads - 1) / threads);
+  for (int z = 0; z < 6; ++z)
+    for (int m = 0; m < nfields_h; ++m) {
+      const int f = fields[m];
+      const int s = c->g.slot[f];
+      if (c->fp32) {
+        const float* src = s < 0 ? nullptr : (const float*)buf + c->g.vol(run, z, s);
+        pack_kernel<float><<<blocks, threads, 0, c->stream>>>(src, c->stage64, c->g);
+      } else {
+        const double* src = s < 0 ? nullptr : (const double*)buf + c->g.vol(run, z, s);
+        pack_kernel<double><<<blocks, threads, 0, c->stream>>>(src, c->stage64, c->g);
+      }
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(host + ((long long)z * nh + m) * V, c->stage64, V * sizeof(double),
+                         cudaMemcpyDeviceToHost, c->stream));
+    }
+  CK(cudaStreamSynchronize(c->stream));
+  return SOLAR_OK;
+}
+
+static const int kAllFields[5] = {kRho, kVxi, kVeta, kVr, kP};
+
+static int check_ctx(solar_ctx* c) {
+  if (!c) return fail(SOLAR_ERR_STATE, "null context");
+  cudaError_t e = cudaSetDevice(c->device);
+  if (e != cudaSuccess) return fail(SOLAR_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
+  return SOLAR_OK;
+}
+
+static int reduce(solar_ctx* c, int run, int sel_field, double* out5) {
+  const int nblocks = 6 * c->g.nr;
+  const int sel = (sel_field >= 0 && sel_field < 5) ? c->g.slot[sel_field] : -1;
+  if (c->fp32)
+    reduce_plane_kernel<float><<<nblocks, 256, 0, c->stream>>>((const float*)c->A, c->g, run, sel, c->dt.rad64,
+                                                               c->dt.vol2, c->dt.drw, c->dt.c2_64, c->part);
+  else
+    reduce_plane_kernel<double><<<nblocks, 256, 0, c->stream>>>((const double*)c->A, c->g, run, sel, c->dt.rad64,
+                                                                c->dt.vol2, c->dt.drw, c->dt.c2_64, c->part);
+  CK(cudaGetLastError());
+  reduce_final_kernel<<<1, 256, 0, c->stream>>>(c->part, nblocks, c->red_out);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out5, c->red_out, 5 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return SOLAR_OK;
+}
+
+}  // namespace solar
+
+// ===================================================================== C-ABI
+extern "C" {
+
+void solar_desc_defaults(solar_desc* d) {
+  if (!d) return;
+  std::memset(d, 0, sizeof(*d));
+  d->precision = SOLAR_FP64;
+  d->nfields = 5;
+  d->nruns = 1;
+  d->sponge_amp = 0.1;
+  d->sponge_exp = 3.0;
+  d->sponge_len = 30;
+  d->sponge_lower = 1;
+  d->sponge_upper = 1;
+}
+
+int solar_gpu_abi_version(void) { return SOLAR_GPU_ABI_VERSION; }
+
+int solar_gpu_last_error(char* buf, int len) {
+  if (!buf || len <= 0) return SOLAR_ERR_ARG;
+  std::snprintf(buf, (size_t)len, "%s", solar::g_last_error.c_str());
+  return SOLAR_OK;
+}
+
+int solar_gpu_finalize(solar_ctx* c) {
+  if (!c) return SOLAR_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
+  if (c->batch_graph) cudaGraphExecDestroy(c->batch_graph);
+  void* ptrs[] = {c->A, c->B, c->W, c->stage64, c->part, c->red_out, c->active, c->target, c->done,
+                  c->dt.rad, c->dt.met, c->dt.conv, c->dt.w9, c->dt.rot, c->dt.c2, c->dt.s0,
+                  c->dt.rad64, c->dt.vol2, c->dt.drw, c->dt.c2_64, c->dt.tanx, c->dt.gr};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  for (auto& e : c->ev)
+    if (e) cudaEventDestroy(e);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return SOLAR_OK;
+}
+
+int solar_gpu_init(const solar_desc* d, solar_ctx** out) {
+  if (!d || !out) return fail(SOLAR_ERR_ARG, "null descriptor or output pointer");
+  *out = nullptr;
+  if (d->precision != SOLAR_FP64 && d->precision != SOLAR_FP32) return fail(SOLAR_ERR_ARG, "precision must be SOLAR_FP64 or SOLAR_FP32");
+  if (d->nfields != 5 && d->nfields != 4) return fail(SOLAR_ERR_ARG, "nfields must be 4 or 5");
+  if (d->nruns < 1) return fail(SOLAR_ERR_ARG, "nruns must be >= 1");
+  if (!(d->dt > 0.0)) return fail(SOLAR_ERR_ARG, "dt must be > 0");
+  solar_ctx* c = new solar_ctx();
+  c->desc = *d;
+  std::string err;
+  int rc = build_tables(*d, c->ht, err);
+  if (rc) { delete c; return fail(rc, "%s", err.c_str()); }
+  if (d->nfields == 4)
+    for (int k = 0; k < d->nr; ++k)
+      if (c->ht.g0[k] != 0.0) { delete c; return fail(SOLAR_ERR_ARG, "nfields = 4 drops rho, which needs g0 == 0"); }
+  c->device = d->device;
+  cudaError_t ce = cudaSetDevice(c->device);
+  if (ce != cudaSuccess) { delete c; return fail(SOLAR_ERR_CUDA, "cudaSetDevice(%d): %s", d->device, cudaGetErrorString(ce)); }
+  c->fp32 = d->precision == SOLAR_FP32;
+  c->esize = c->fp32 ? 4 : 8;
+  Geom& g = c->g;
+  g.n = d->nx;
+  g.nr = d->nr;
+  g.nf = d->nfields;
+  g.pitch = d->nx + 2 * IOFF;
+  g.rows = d->nx + 2 * JOFF;
+  g.plane = (long long)g.pitch * g.rows;
+  g.vs = ((g.plane * g.nr + 63) / 64) * 64;
+  g.nruns = d->nruns;
+  if (g.nf == 5) { for (int f = 0; f < 5; ++f) g.slot[f] = f; }
+  else { g.slot[kRho] = -1; g.slot[kVxi] = 0; g.slot[kVeta] = 1; g.slot[kVr] = 2; g.slot[kP] = 3; }
+  // tile choice
+  c->tile_x = d->tile_x ? d->tile_x : (g.n % 32 == 0 ? 32 : 16);
+  c->tile_y = d->tile_y ? d->tile_y : 8;
+  if (g.n % c->tile_x || g.n % c->tile_y) { solar_gpu_finalize(c); return fail(SOLAR_ERR_ARG, "tile does not divide nx"); }
+  if (d->kchunk > 0) c->kchunk = d->kchunk;
+  else {
+    const long long blocks = 6LL * g.nruns * (g.n / c->tile_x) * (g.n / c->tile_y);
+    const long long want = 148LL * 6;
+    int nch = (int)std::max<long long>(1, (want + blocks - 1) / blocks);
+    c->kchunk = std::max(8, (g.nr + nch - 1) / nch);
+  }
+#define TRY(x) do { int rc_ = (x); if (rc_) { solar_gpu_finalize(c); return rc_; } } while (0)
+#define TRYC(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) { std::string m_ = cudaGetErrorString(e_); solar_gpu_finalize(c); return fail(e_ == cudaErrorMemoryAllocation ? SOLAR_ERR_NOMEM : SOLAR_ERR_CUDA, "%s: %s", #call, m_.c_str()); } } while (0)
+  TRYC(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  const size_t bytes = (size_t)g.nruns * 6 * g.nf * g.vs * c->esize;
+  TRYC(cudaMalloc(&c->A, bytes));
+  TRYC(cudaMalloc(&c->B, bytes));
+  TRYC(cudaMalloc(&c->W, bytes));
+  TRYC(cudaMemset(c->A, 0, bytes));
+  TRYC(cudaMemset(c->B, 0, bytes));
+  TRYC(cudaMemset(c->W, 0, bytes));
+  TRYC(cudaMalloc((void**)&c->stage64, (size_t)vol_compact(c) * sizeof(double)));
+  TRYC(cudaMalloc((void**)&c->part, (size_t)6 * g.nr * 5 * sizeof(double)));
+  TRYC(cudaMalloc((void**)&c->red_out, 5 * sizeof(double)));
+  TRYC(cudaMalloc((void**)&c->active, g.nruns * sizeof(int)));
+  TRYC(cudaMalloc((void**)&c->target, g.nruns * sizeof(int)));
+  TRYC(cudaMalloc((void**)&c->done, g.nruns * sizeof(int)));
+  TRY(upload_constants());
+  if (c->fp32) TRY(upload_tables<float>(c));
+  else TRY(upload_tables<double>(c));
+  TRYC(cudaMalloc((void**)&c->dt.s0, c->ht.s0.size() * sizeof(int)));
+  TRYC(cudaMemcpy(c->dt.s0, c->ht.s0.data(), c->ht.s0.size() * sizeof(int), cudaMemcpyHostToDevice));
+  TRY(upload<double>((void**)&c->dt.rad64, c->ht.radial));
+  {
+    std::vector<double> vol2(c->ht.metric.begin() + (size_t)kMVol * g.n * g.n,
+                             c->ht.metric.begin() + (size_t)(kMVol + 1) * g.n * g.n);
+    TRY(upload<double>((void**)&c->dt.vol2, vol2));
+  }
+  TRY(upload<double>((void**)&c->dt.drw, c->ht.dr_weight));
+  TRY(upload<double>((void**)&c->dt.tanx, c->ht.tanx));
+  TRY(upload<double>((void**)&c->dt.gr, c->ht.gr));
+  if (d->c2_3d) {
+    std::vector<double> c2(d->c2_3d, d->c2_3d + (size_t)6 * vol_compact(c));
+    TRY(upload<double>((void**)&c->dt.c2_64, c2));
+    if (c->fp32) TRY(upload<float>(&c->dt.c2, c2));
+    else TRY(upload<double>(&c->dt.c2, c2));
+  }
+  for (auto& e : c->ev) TRYC(cudaEventCreate(&e));
+  TRYC(cudaStreamSynchronize(c->stream));
+#undef TRY
+#undef TRYC
+  *out = c;
+  return SOLAR_OK;
+}
+
+int solar_gpu_set_state(solar_ctx* c, int run, const double* q) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!q || run < 0 || run >= c->g.nruns) return fail(SOLAR_ERR_ARG, "bad run or null state");
+  if ((rc = upload_fields(c, c->A, run, q, 5, kAllFields, 5))) return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  return SOLAR_OK;
+}
+
+int solar_gpu_get_state(solar_ctx* c, int run, double* q) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!q || run < 0 || run >= c->g.nruns) return fail(SOLAR_ERR_ARG, "bad run or null state");
+  return download_fields(c, c->A, run, q, 5, kAllFields, 5);
+}
+
+int solar_gpu_add_gaussian(solar_ctx* c, int run, double x0, double y0, double z0, double width,
+                           double amp) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (run < 0 || run >= c->g.nruns || !(width > 0.0)) return fail(SOLAR_ERR_ARG, "bad run or width");
+  // face by face: pressure volume -> compact FP64 scratch, add the pulse, write back
+  const long long V = vol_compact(c);
+  const int threads = 256, blocks = (int)((V + threads - 1) / threads);
+  const int s = c->g.slot[kP];
+  for (int z = 0; z < 6; ++z) {
+    const long long off = c->g.vol(run, z, s);
+    if (c->fp32) pack_kernel<float><<<blocks, threads, 0, c->stream>>>((const float*)c->A + off, c->stage64, c->g);
+    else pack_kernel<double><<<blocks, threads, 0, c->stream>>>((const double*)c->A + off, c->stage64, c->g);
+    gaussian_kernel<<<blocks, threads, 0, c->stream>>>(c->stage64, c->g, z, c->dt.tanx, c->dt.gr, x0, y0, z0,
+                                                       width, amp);
+    if (c->fp32) unpack_kernel<float><<<blocks, threads, 0, c->stream>>>(c->stage64, (float*)c->A + off, c->g);
+    else unpack_kernel<double><<<blocks, threads, 0, c->stream>>>(c->stage64, (double*)c->A + off, c->g);
+    CK(cudaGetLastError());
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return SOLAR_OK;
+}
+
+int solar_gpu_rk4(solar_ctx* c, int nsteps) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (nsteps < 0) return fail(SOLAR_ERR_ARG, "nsteps < 0");
+  if ((rc = capture_step_graph(c))) return rc;
+  for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(c->step_graph, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return SOLAR_OK;
+}
+
+int solar_gpu_rk4_runs(solar_ctx* c, const int* nsteps_per_run) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!nsteps_per_run) return fail(SOLAR_ERR_ARG, "null step counts");
+  const int R = c->g.nruns;
+  int maxs = 0;
+  for (int r = 0; r < R; ++r) {
+    if (nsteps_per_run[r] < 0) return fail(SOLAR_ERR_ARG, "negative step count");
+    maxs = std::max(maxs, nsteps_per_run[r]);
+  }
+  CK(cudaMemcpyAsync(c->target, nsteps_per_run, R * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemsetAsync(c->done, 0, R * sizeof(int), c->stream));
+  if ((rc = capture_batch_graph(c))) return rc;
+  for (int s = 0; s < maxs; ++s) CK(cudaGraphLaunch(c->batch_graph, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return SOLAR_OK;
+}
+
+// Operator-level drop-ins: inputs go to buffer B (run 0), results come from buffer W.
+// The state buffer A is left untouched.
+static int op_prepare_state(solar_ctx* c, const double* q) {
+  int rc = upload_fields(c, c->B, 0, q, 5, kAllFields, 5);
+  return rc;
+}
+
+int solar_gpu_compute_rhs(solar_ctx* c, const double* q, double* rhs) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!q || !rhs) return fail(SOLAR_ERR_ARG, "null array");
+  if ((rc = op_prepare_state(c, q))) return rc;
+  if (c->fp32) { launch_edge<float>(c, c->B, 0, nullptr); launch_stage<float>(c, c->B, c->W, 2, 0, nullptr); }
+  else { launch_edge<double>(c, c->B, 0, nullptr); launch_stage<double>(c, c->B, c->W, 2, 0, nullptr); }
+  CK(cudaGetLastError());
+  return download_fields(c, c->W, 0, rhs, 5, kAllFields, 5);
+}
+
+static int bc_sponge_op(solar_ctx* c, const double* q, double* rhs, int do_bc, int do_sponge) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!rhs || (do_sponge && !q)) return fail(SOLAR_ERR_ARG, "null array");
+  if ((rc = upload_fields(c, c->W, 0, rhs, 5, kAllFields, 5))) return rc;
+  if (q && (rc = upload_fields(c, c->B, 0, q, 5, kAllFields, 5))) return rc;
+  const long long n6 = 6 * vol_compact(c);
+  const int threads = 256, blocks = (int)((n6 + threads - 1) / threads);
+  if (c->fp32) bc_sponge_kernel<float><<<blocks, threads, 0, c->stream>>>((float*)c->W, (const float*)c->B, (const float*)c->dt.rad, c->g, 0, do_bc, do_sponge);
+  else bc_sponge_kernel<double><<<blocks, threads, 0, c->stream>>>((double*)c->W, (const double*)c->B, (const double*)c->dt.rad, c->g, 0, do_bc, do_sponge);
+  CK(cudaGetLastError());
+  return download_fields(c, c->W, 0, rhs, 5, kAllFields, 5);
+}
+
+int solar_gpu_bc_rhs(solar_ctx* c, double* rhs) { return bc_sponge_op(c, nullptr, rhs, 1, 0); }
+int solar_gpu_sponge(solar_ctx* c, const double* q, double* rhs) { return bc_sponge_op(c, q, rhs, 0, 1); }
+
+int solar_gpu_filter_exp(solar_ctx* c, const double* q, double* qf) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!q || !qf) return fail(SOLAR_ERR_ARG, "null array");
+  if ((rc = op_prepare_state(c, q))) return rc;
+  if (c->fp32) { launch_edge<float>(c, c->B, 1, nullptr); launch_filter<float>(c, c->B, c->W, nullptr); }
+  else { launch_edge<double>(c, c->B, 1, nullptr); launch_filter<double>(c, c->B, c->W, nullptr); }
+  CK(cudaGetLastError());
+  return download_fields(c, c->W, 0, qf, 5, kAllFields, 5);
+}
+
+static int grad_div_op(solar_ctx* c, const double* fields[4], double* outs[4]) {
+  // fields: v_xi, v_eta, v_r, p (any may be null -> zero); outs: grad_xi, grad_eta, grad_r, div
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  const long long n6 = 6 * vol_compact(c);
+  std::vector<double> q((size_t)5 * n6, 0.0);
+  const long long V = vol_compact(c);
+  const int ref[4] = {kVxi, kVeta, kVr, kP};
+  for (int m = 0; m < 4; ++m)
+    if (fields[m])
+      for (int z = 0; z < 6; ++z)
+        std::memcpy(&q[((size_t)z * 5 + ref[m]) * V], fields[m] + (size_t)z * V, V * sizeof(double));
+  if ((rc = op_prepare_state(c, q.data()))) return rc;
+  if (c->fp32) { launch_edge<float>(c, c->B, 0, nullptr); launch_stage<float>(c, c->B, c->W, 3, 0, nullptr); }
+  else { launch_edge<double>(c, c->B, 0, nullptr); launch_stage<double>(c, c->B, c->W, 3, 0, nullptr); }
+  CK(cudaGetLastError());
+  for (int m = 0; m < 4; ++m) {
+    if (!outs[m]) continue;
+    const int f = ref[m];
+    if ((rc = download_fields(c, c->W, 0, outs[m], 1, &f, 1))) return rc;
+  }
+  return SOLAR_OK;
+}
+
+int solar_gpu_gradient(solar_ctx* c, const double* p, double* gxi, double* geta, double* gr) {
+  if (!p) return fail(SOLAR_ERR_ARG, "null array");
+  const double* f[4] = {nullptr, nullptr, nullptr, p};
+  double* o[4] = {gxi, geta, gr, nullptr};
+  return grad_div_op(c, f, o);
+}
+
+int solar_gpu_divergence(solar_ctx* c, const double* vxi, const double* veta, const double* vr, double* div) {
+  if (!vxi || !veta || !vr || !div) return fail(SOLAR_ERR_ARG, "null array");
+  const double* f[4] = {vxi, veta, vr, nullptr};
+  double* o[4] = {nullptr, nullptr, nullptr, div};
+  return grad_div_op(c, f, o);
+}
+
+int solar_gpu_norm(solar_ctx* c, int run, int field, double* out) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!out || field < 1 || field > 5 || run < 0 || run >= c->g.nruns) return fail(SOLAR_ERR_ARG, "bad field/run");
+  double r[5];
+  if ((rc = reduce(c, run, field - 1, r))) return rc;
+  // auxiliary.f90:122
+  *out = std::pow(r[0] / ((double)c->g.n * c->g.n * c->g.nr) * 6.0, 0.5);
+  return SOLAR_OK;
+}
+
+int solar_gpu_diag(solar_ctx* c, int run, double* out4) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!out4 || run < 0 || run >= c->g.nruns) return fail(SOLAR_ERR_ARG, "bad run");
+  double r[5];
+  if ((rc = reduce(c, run, -1, r))) return rc;
+  out4[0] = r[1];
+  out4[1] = r[2];
+  out4[2] = r[3];
+  out4[3] = r[4] > 0 ? 1.0 : 0.0;
+  return SOLAR_OK;
+}
+
+int solar_gpu_time_rk4(solar_ctx* c, int nsteps, int per_kernel, double* out7) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!out7 || nsteps < 1) return fail(SOLAR_ERR_ARG, "bad arguments");
+  for (int m = 0; m < 7; ++m) out7[m] = 0.0;
+  if (!per_kernel) {
+    if ((rc = capture_step_graph(c))) return rc;
+    CK(cudaEventRecord(c->ev[0], c->stream));
+    for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(c->step_graph, c->stream));
+    CK(cudaEventRecord(c->ev[1], c->stream));
+    CK(cudaEventSynchronize(c->ev[1]));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
+    out7[0] = ms;
+    return SOLAR_OK;
+  }
+  std::vector<cudaEvent_t> evs;
+  CK(cudaEventRecord(c->ev[0], c->stream));
+  for (int s = 0; s < nsteps; ++s) enqueue_step_any(c, nullptr, &evs);
+  CK(cudaEventRecord(c->ev[1], c->stream));
+  CK(cudaEventSynchronize(c->ev[1]));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
+  out7[0] = ms;
+  // event layout per step: [e, edge, e, stage, e] x5 then [e, edge, e, filter, e]
+  // marks are recorded around every launch: pairs (0,1)=edge, (1,2)=stage, ... per stage
+  const size_t per_step = 18;
+  for (size_t s = 0; s + per_step <= evs.size(); s += per_step) {
+    for (int st = 0; st < 5; ++st) {
+      float a = 0, b = 0;
+      cudaEventElapsedTime(&a, evs[s + st * 3 + 0], evs[s + st * 3 + 1]);
+      cudaEventElapsedTime(&b, evs[s + st * 3 + 1], evs[s + st * 3 + 2]);
+      out7[3] += a;
+      out7[1] += b;
+      out7[6] += 1;
+      out7[4] += 1;
+    }
+    float a = 0, b = 0;
+    cudaEventElapsedTime(&a, evs[s + 15], evs[s + 16]);
+    cudaEventElapsedTime(&b, evs[s + 16], evs[s + 17]);
+    out7[3] += a;
+    out7[2] += b;
+    out7[6] += 1;
+    out7[5] += 1;
+  }
+  for (auto e : evs) cudaEventDestroy(e);
+  if (out7[4] > 0) out7[1] /= out7[4];
+  if (out7[5] > 0) out7[2] /= out7[5];
+  if (out7[6] > 0) out7[3] /= out7[6];
+  return SOLAR_OK;
+}
+
+int solar_gpu_synchronize(solar_ctx* c) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  return SOLAR_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,189 @@
+"""Host-side mirror of the reference's time-stepping call surface.
+
+The reference (Fortran 90 + MPI) exposes its hot path as the subroutines ``RK4``
+(timestep.f90:41), ``COMPUTE_RHS`` (compute_rhs_acoustic.f90:1), ``BC_RHS``
+(bc_acoustic_wave.f90:1), ``SPONGE`` (sponge.f90:1), ``FILTER_EXP`` (filter.f90:9),
+``COMPUTE_GRADIENT`` / ``COMPUTE_DIVERGENCE`` (grad.f90:13, 62) and the diagnostic
+``norm`` (auxiliary.f90:100).  :class:`Solver` offers the same operations, with the same
+array meaning, over the C-ABI of ``include/solar_gpu.h``.  Arrays are numpy float64 in
+"six-zone Fortran order": a field is ``f[zone, k, j, i]`` and a state is
+``q[zone, m, k, j, i]`` with m = rho, v_xi, v_eta, v_r, p -- the reference's per-zone
+arrays ``f(mx,my,mr)`` / ``q(mx,my,mr,5)`` stacked over the six zones.
+
+Errors from the library raise :class:`solar_b200._lib.SolarError`; there is no CPU
+fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Iterable, Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from .configs import Config, Source
+
+_D = ctypes.POINTER(ctypes.c_double)
+
+
+def _ptr(a: np.ndarray):
+    if a.dtype != np.float64 or not a.flags.c_contiguous:
+        raise TypeError("arrays must be C-contiguous float64")
+    return a.ctypes.data_as(_D)
+
+
+class Solver:
+    """One GPU context holding ``nruns`` independent six-face runs of one grid."""
+
+    def __init__(self, cfg: Config, precision: str = "fp64", nfields: int = 5, nruns: int = 1,
+                 device: int = 0, fix_reversed_rotation: bool = False,
+                 c2_3d: Optional[np.ndarray] = None, tile: Optional[Sequence[int]] = None):
+        self.lib = _lib.load()
+        self.cfg = cfg
+        self.nx, self.nr = cfg.nx, cfg.nr
+        self.nruns = nruns
+        self.nfields = nfields
+        self.precision = precision
+        d = _lib.SolarDesc()
+        self.lib.solar_desc_defaults(ctypes.byref(d))
+        self._model = np.ascontiguousarray(cfg.model, dtype=np.float64)
+        self._c2 = None if c2_3d is None else np.ascontiguousarray(c2_3d, dtype=np.float64)
+        d.nx, d.nr = cfg.nx, cfg.nr
+        d.precision = {"fp64": _lib.SOLAR_FP64, "fp32": _lib.SOLAR_FP32}[precision]
+        d.nfields = nfields
+        d.nruns = nruns
+        d.device = device
+        d.dt = float(cfg.dt)
+        d.model = _ptr(self._model)
+        d.c2_3d = _ptr(self._c2) if self._c2 is not None else None
+        sp = cfg.sponge
+        d.sponge_amp, d.sponge_exp, d.sponge_len = float(sp.amp), float(sp.exp), int(sp.length)
+        d.sponge_lower, d.sponge_upper = int(sp.lower), int(sp.upper)
+        d.fix_reversed_rotation = int(bool(fix_reversed_rotation))
+        if tile is not None:
+            d.tile_x, d.tile_y, d.kchunk = (list(tile) + [0, 0, 0])[:3]
+        self.desc = d
+        h = ctypes.c_void_p()
+        _lib.check(self.lib.solar_gpu_init(ctypes.byref(d), ctypes.byref(h)))
+        self._h = h
+
+    # ------------------------------------------------------------------ lifetime
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self.lib.solar_gpu_finalize(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ------------------------------------------------------------------ shapes
+    @property
+    def field_shape(self):
+        return (6, self.nr, self.nx, self.nx)
+
+    @property
+    def state_shape(self):
+        return (6, 5, self.nr, self.nx, self.nx)
+
+    @property
+    def points(self) -> int:
+        return 6 * self.nx * self.nx * self.nr
+
+    # ------------------------------------------------------------------ state (COMMON /RKWORK/ q)
+    def set_state(self, q: np.ndarray, run: int = 0) -> None:
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        if q.shape != self.state_shape:
+            raise ValueError(f"state shape {q.shape} != {self.state_shape}")
+        _lib.check(self.lib.solar_gpu_set_state(self._h, run, _ptr(q)))
+
+    def get_state(self, run: int = 0, out: Optional[np.ndarray] = None) -> np.ndarray:
+        q = np.empty(self.state_shape) if out is None else out
+        _lib.check(self.lib.solar_gpu_get_state(self._h, run, _ptr(q)))
+        return q
+
+    def add_gaussian(self, src: Source, run: int = 0) -> None:
+        x0, y0, z0 = map(float, src.x0)
+        _lib.check(self.lib.solar_gpu_add_gaussian(self._h, run, x0, y0, z0, float(src.width), float(src.amp)))
+
+    def init_sources(self, sources: Optional[Iterable[Source]] = None, run: int = 0) -> None:
+        """GENERATE_IC slot: zero state plus the configuration's Gaussian pulses."""
+        self.set_state(np.zeros(self.state_shape), run)
+        for s in (self.cfg.sources if sources is None else sources):
+            self.add_gaussian(s, run)
+
+    # ------------------------------------------------------------------ time stepping
+    def rk4(self, nsteps: int = 1) -> None:
+        """``nsteps`` calls of the reference's RK4 (timestep.f90:41-86) on every run."""
+        _lib.check(self.lib.solar_gpu_rk4(self._h, int(nsteps)))
+
+    def rk4_runs(self, steps: Sequence[int]) -> None:
+        """Advance run r by steps[r] RK4 steps (uneven counts, one batched graph)."""
+        s = np.ascontiguousarray(np.asarray(steps, dtype=np.int32))
+        if s.shape != (self.nruns,):
+            raise ValueError("need one step count per run")
+        _lib.check(self.lib.solar_gpu_rk4_runs(self._h, s.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
+
+    # ------------------------------------------------------------------ operators
+    def compute_rhs(self, q: np.ndarray) -> np.ndarray:
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        rhs = np.empty(self.state_shape)
+        _lib.check(self.lib.solar_gpu_compute_rhs(self._h, _ptr(q), _ptr(rhs)))
+        return rhs
+
+    def bc_rhs(self, rhs: np.ndarray) -> np.ndarray:
+        out = np.ascontiguousarray(rhs, dtype=np.float64).copy()
+        _lib.check(self.lib.solar_gpu_bc_rhs(self._h, _ptr(out)))
+        return out
+
+    def sponge(self, q: np.ndarray, rhs: np.ndarray) -> np.ndarray:
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        out = np.ascontiguousarray(rhs, dtype=np.float64).copy()
+        _lib.check(self.lib.solar_gpu_sponge(self._h, _ptr(q), _ptr(out)))
+        return out
+
+    def filter_exp(self, q: np.ndarray) -> np.ndarray:
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        qf = np.empty(self.state_shape)
+        _lib.check(self.lib.solar_gpu_filter_exp(self._h, _ptr(q), _ptr(qf)))
+        return qf
+
+    def gradient(self, p: np.ndarray):
+        p = np.ascontiguousarray(p, dtype=np.float64)
+        gx, ge, gr = (np.empty(self.field_shape) for _ in range(3))
+        _lib.check(self.lib.solar_gpu_gradient(self._h, _ptr(p), _ptr(gx), _ptr(ge), _ptr(gr)))
+        return gx, ge, gr
+
+    def divergence(self, vxi: np.ndarray, veta: np.ndarray, vr: np.ndarray) -> np.ndarray:
+        a = [np.ascontiguousarray(x, dtype=np.float64) for x in (vxi, veta, vr)]
+        out = np.empty(self.field_shape)
+        _lib.check(self.lib.solar_gpu_divergence(self._h, _ptr(a[0]), _ptr(a[1]), _ptr(a[2]), _ptr(out)))
+        return out
+
+    # ------------------------------------------------------------------ diagnostics
+    def norm(self, field: int = 4, run: int = 0) -> float:
+        out = ctypes.c_double()
+        _lib.check(self.lib.solar_gpu_norm(self._h, run, field, ctypes.byref(out)))
+        return out.value
+
+    def diag(self, run: int = 0) -> dict:
+        out = (ctypes.c_double * 4)()
+        _lib.check(self.lib.solar_gpu_diag(self._h, run, out))
+        return {"energy": out[0], "mass": out[1], "max_abs_p": out[2], "nonfinite": bool(out[3])}
+
+    def time_rk4(self, nsteps: int, per_kernel: bool = False) -> dict:
+        out = (ctypes.c_double * 7)()
+        _lib.check(self.lib.solar_gpu_time_rk4(self._h, int(nsteps), int(per_kernel), out))
+        return {"total_ms": out[0], "stage_ms": out[1], "filter_ms": out[2], "edge_ms": out[3],
+                "stage_launches": int(out[4]), "filter_launches": int(out[5]), "edge_launches": int(out[6])}
+
+    def synchronize(self) -> None:
+        _lib.check(self.lib.solar_gpu_synchronize(self._h))

@@ -1,0 +1,230 @@
+"""GPU parity against the FP64 oracle, through the C-ABI.
+
+Tolerances (relative L2 per field, ||gpu - oracle|| / ||oracle||):
+  * FP64 operators (gradient, divergence, COMPUTE_RHS, BC_RHS, SPONGE, FILTER_EXP): 1e-12
+  * FP64 time stepping, 100 steps: 1e-11
+  * FP32 time stepping against the FP64 oracle: 1e-5 (precision-path target)
+"""
+import numpy as np
+import pytest
+
+from solar_b200 import configs
+from solar_b200.solver import Solver
+from tests import geometry as G
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("rho", "v_xi", "v_eta", "v_r", "p")
+
+
+def rel_l2(a, b):
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / (nb if nb > 0 else 1.0)
+
+
+def per_field(a, b, fields=range(5)):
+    return {FIELDS[m]: rel_l2(a[:, m], b[:, m]) for m in fields}
+
+
+@pytest.fixture(scope="module")
+def c1_small():
+    return configs.c1(nx=32, nr=32)
+
+
+@pytest.fixture(scope="module")
+def c2_small():
+    return configs.c2(nx=32, nr=32, nsteps=100)
+
+
+def random_state(shape, seed):
+    rng = np.random.default_rng(seed)
+    return rng.standard_normal(shape)
+
+
+def smooth_state(o, seed):
+    """A state whose five fields are sums of seeded Gaussian blobs (smooth, nonzero
+    everywhere that matters)."""
+    rng = np.random.default_rng(seed)
+    q = np.zeros(o.state_shape)
+    for m in range(5):
+        for _ in range(3):
+            d = rng.standard_normal(3)
+            d = d / np.linalg.norm(d) * rng.uniform(0.6, 0.95)
+            src = configs.Source(tuple(d), 0.08, rng.uniform(0.5, 1.5))
+            g = o.initial_state([src])[:, 4]
+            q[:, m] += g
+    return q
+
+
+# ---------------------------------------------------------------- operators, FP64
+def test_state_roundtrip_fp64(oracle_mod, c1_small):
+    with Solver(c1_small) as s:
+        q = random_state(s.state_shape, 1)
+        s.set_state(q)
+        assert np.array_equal(s.get_state(), q)
+
+
+def test_gaussian_ic_matches_oracle(oracle_mod, c1_small):
+    o = oracle_mod.Oracle(c1_small)
+    with Solver(c1_small) as s:
+        s.init_sources()
+        assert rel_l2(s.get_state()[:, 4], o.initial_state()[:, 4]) < 1e-12
+
+
+@pytest.mark.parametrize("cfgname", ["c1_small", "c2_small"])
+def test_gradient_and_divergence_fp64(oracle_mod, cfgname, request):
+    cfg = request.getfixturevalue(cfgname)
+    o = oracle_mod.Oracle(cfg)
+    q = smooth_state(o, 2)
+    with Solver(cfg) as s:
+        g_gpu = s.gradient(q[:, 4])
+        g_ref = o.gradient(q[:, 4])
+        for a, b in zip(g_gpu, g_ref):
+            assert rel_l2(a, b) < 1e-12
+        d_gpu = s.divergence(q[:, 1], q[:, 2], q[:, 3])
+        d_ref = o.divergence(q[:, 1], q[:, 2], q[:, 3])
+        assert rel_l2(d_gpu, d_ref) < 1e-12
+
+
+def test_divergence_fixed_rotation_option(oracle_mod, c1_small):
+    o = oracle_mod.Oracle(c1_small, fix_reversed_rotation=True)
+    vxi, veta = G.rotation_field(c1_small.nx, o.grid(3))
+    vr = np.zeros_like(vxi)
+    with Solver(c1_small, fix_reversed_rotation=True) as s:
+        d = s.divergence(vxi, veta, vr)
+    assert rel_l2(d, o.divergence(vxi, veta, vr)) < 1e-12 or np.abs(d - o.divergence(vxi, veta, vr)).max() < 1e-12
+    assert max(G.edge_maxima(d).values()) < 1e-4
+
+
+@pytest.mark.parametrize("cfgname", ["c1_small", "c2_small"])
+def test_compute_rhs_bc_sponge_fp64(oracle_mod, cfgname, request):
+    cfg = request.getfixturevalue(cfgname)
+    o = oracle_mod.Oracle(cfg)
+    q = smooth_state(o, 3)
+    with Solver(cfg) as s:
+        rhs = s.compute_rhs(q)
+        ref = o.compute_rhs(q)
+        for name, e in per_field(rhs, ref).items():
+            assert e < 1e-12, (name, e)
+        bc = s.bc_rhs(ref)
+        assert np.array_equal(bc, o.bc_rhs(ref))
+        sp = s.sponge(q, ref)
+        assert np.abs(sp - o.sponge(q, ref)).max() <= 1e-14 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("cfgname", ["c1_small", "c2_small"])
+def test_filter_exp_fp64(oracle_mod, cfgname, request):
+    cfg = request.getfixturevalue(cfgname)
+    o = oracle_mod.Oracle(cfg)
+    q = smooth_state(o, 4)
+    with Solver(cfg) as s:
+        qf = s.filter_exp(q)
+    ref = o.filter_exp(q)
+    for name, e in per_field(qf, ref).items():
+        assert e < 1e-12, (name, e)
+    assert np.all(qf[:, :, :5] == 0) and np.all(qf[:, :, -5:] == 0)
+
+
+def test_filter_exp_random_fields_fp64(oracle_mod, c1_small):
+    """Rough input: every halo value matters at full weight."""
+    o = oracle_mod.Oracle(c1_small)
+    q = random_state(o.state_shape, 5)
+    with Solver(c1_small) as s:
+        qf = s.filter_exp(q)
+        rhs = s.compute_rhs(q)
+    for name, e in per_field(qf, o.filter_exp(q)).items():
+        assert e < 1e-12, (name, e)
+    for name, e in per_field(rhs, o.compute_rhs(q)).items():
+        assert e < 1e-12, (name, e)
+
+
+# ---------------------------------------------------------------- time stepping
+def test_rk4_c1_100_steps_fp64(oracle_mod, c1_small):
+    """Config 1 (6 x 32^3, 100 steps): per-field relative L2 <= 1e-11."""
+    o = oracle_mod.Oracle(c1_small)
+    q0 = o.initial_state()
+    ref = o.rk4(q0, 100)
+    with Solver(c1_small) as s:
+        s.set_state(q0)
+        s.rk4(100)
+        q = s.get_state()
+        assert abs(s.norm(4) - o.norm(ref, 4)) <= 1e-11 * o.norm(ref, 4)
+    for name, e in per_field(q, ref).items():
+        assert e < 1e-11, (name, e)
+
+
+def test_rk4_stratified_fp64_and_fp32(oracle_mod, c2_small):
+    """Stratified shell at 6 x 32^3, 100 steps: FP64 <= 1e-11; FP32 (4 fields) <= 1e-5."""
+    o = oracle_mod.Oracle(c2_small)
+    q0 = o.initial_state()
+    ref = o.rk4(q0, 100)
+    with Solver(c2_small) as s:
+        s.set_state(q0)
+        s.rk4(100)
+        for name, e in per_field(s.get_state(), ref).items():
+            assert e < 1e-11, (name, e)
+    with Solver(c2_small, precision="fp32", nfields=4) as s:
+        s.set_state(q0)
+        s.rk4(100)
+        q = s.get_state()
+        assert np.all(q[:, 0] == 0)
+        for name, e in per_field(q, ref, fields=(1, 2, 3, 4)).items():
+            assert e < 1e-5, (name, e)
+
+
+def test_rk4_fp32_five_fields_c1(oracle_mod, c1_small):
+    o = oracle_mod.Oracle(c1_small)
+    q0 = o.initial_state()
+    ref = o.rk4(q0, 100)
+    with Solver(c1_small, precision="fp32") as s:
+        s.set_state(q0)
+        s.rk4(100)
+        for name, e in per_field(s.get_state(), ref, fields=(1, 2, 3, 4)).items():
+            assert e < 1e-5, (name, e)
+
+
+def test_graph_and_direct_launch_agree(c1_small):
+    with Solver(c1_small) as s:
+        s.init_sources()
+        q0 = s.get_state()
+        s.rk4(3)
+        a = s.get_state()
+        s.set_state(q0)
+        s.time_rk4(3, per_kernel=True)
+        b = s.get_state()
+    assert np.array_equal(a, b)
+
+
+def test_batched_uneven_runs_match_single_runs(c1_small):
+    steps = [3, 7, 0, 5]
+    srcs = [configs.Source((0.0, 0.0, 0.75), 0.05, 1.0), configs.Source((0.75, 0.0, 0.0), 0.04, 0.5),
+            configs.Source((0.0, -0.7, 0.2), 0.06, 2.0), configs.Source((0.3, 0.3, -0.6), 0.05, 1.0)]
+    with Solver(c1_small, nruns=4) as b:
+        for r, src in enumerate(srcs):
+            b.init_sources([src], run=r)
+        b.rk4_runs(steps)
+        got = [b.get_state(r) for r in range(4)]
+    with Solver(c1_small) as s:
+        for r, src in enumerate(srcs):
+            s.init_sources([src])
+            s.rk4(steps[r])
+            assert np.array_equal(s.get_state(), got[r]), r
+
+
+def test_norm_and_diag(oracle_mod, c1_small):
+    o = oracle_mod.Oracle(c1_small)
+    q = smooth_state(o, 6)
+    with Solver(c1_small) as s:
+        s.set_state(q)
+        for m in range(1, 6):
+            assert abs(s.norm(m) - o.norm(q, m)) <= 1e-12 * o.norm(q, m)
+        d = s.diag()
+        assert d["energy"] > 0 and not d["nonfinite"]
+        assert d["max_abs_p"] == pytest.approx(np.abs(q[:, 4]).max(), rel=1e-15)
+
+
+def test_bad_run_index_raises(c1_small):
+    from solar_b200._lib import SolarError
+    with Solver(c1_small) as s:
+        with pytest.raises(SolarError):
+            s.get_state(run=3)
