@@ -19,6 +19,8 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 
+#include "tma.cuh"
+
 namespace solar {
 
 constexpr int IOFF = 8;   // interior column offset inside a padded row
@@ -69,22 +71,24 @@ template <> struct Coef<float> {
 };
 
 // ---------------------------------------------------------------------------------
-// Edge (ghost) kernel: INTERPOLATE_ALONG_X/Y + TRANSFORM_VECTOR_BETWEEN_MESHES_DIV +
-// the inter-zone exchange and its reversal, all in one pass.  One thread computes one
-// ghost value (receiver face, edge, layer, k, position along the edge) by a 9-tap
-// Lagrange sum over the source face's plane 1+layer / n-2-layer.
-// mode 0: RHS halos -- p scalar on all edges; v_xi rotated on W/E; v_eta rotated on S/N.
+// Edge (ghost) kernel: INTERPOLATE_ALONG_X/Y + TRANSFORM_VECTOR_BETWEEN_MESHES_DIV + the
+// inter-zone exchange and its reversal, in one pass.  Each thread owns one ghost point
+// (receiver face, edge, layer, position along the edge) and walks a chunk of radial planes.
+// Its 9 source points and coefficients are loaded once: the scalar weights are the
+// Lagrange weights; the vector coefficients fold the Lagrange weight, the source face's
+// (xi,eta)->(theta,phi) conversion and the receiver-frame rotation into one pair per tap.
+// mode 0: RHS halos -- p scalar on all edges; v_xi on W/E and v_eta on S/N, rotated.
 // mode 1: filter halos -- every stored field, scalar, all edges (filter.f90:23-28).
 template <typename T>
 struct EdgeArgs {
-  T* q;                     // buffer whose frames are filled (interior is the source)
-  const T* w9;              // [3][n][9]
-  const int* s0;            // [3][n]
-  const T* conv;            // [3 kinds][4][n][n]
-  const T* rot;             // [6][4][3][n][2]
+  T* q;                     // buffer whose frames are filled (its interior is the source)
+  const T* ew;              // [6][4][3][n][9]
+  const T* eg;              // [6][4][3][n][9][2]
+  const int* esrc;          // [6][4][3][n][9]  source point j*n + i
   const int* active;        // per-run flag or nullptr
   Geom g;
   int mode;
+  int kchunk;
 };
 
 template <typename T>
@@ -93,97 +97,132 @@ __global__ void __launch_bounds__(192) edge_kernel(const EdgeArgs<T> a) {
   const int n = g.n;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;   // position along the edge
   const int l = threadIdx.y;                             // ghost layer 0..2
-  const int k = blockIdx.y;
   const int z = blockIdx.z;                              // (run*6 + face)*4 + edge
   const int e = z & 3, face = (z >> 2) % 6, run = (z >> 2) / 6;
   if (t >= n) return;
   if (a.active && !a.active[run]) return;
+  const int kb = blockIdx.y * a.kchunk;
+  const int ke = min(g.nr, kb + a.kchunk);
   const EdgeRouteDev rt = cRoute[face][e];
-  const int ts = rt.reversed ? n - 1 - t : t;
-  const int s0 = a.s0[l * n + ts];
-  const T* w = a.w9 + ((long long)l * n + ts) * 9;
-  // source points: along i on row js (S/N strips) or along j on column is (W/E strips)
-  const bool along_i = rt.src_edge <= 1;
-  const int fixed = (rt.src_edge == 0 || rt.src_edge == 2) ? l + 1 : n - 2 - l;
-  long long src_off[9];
-  int src_p2[9];
+  const long long row = ((((long long)face * 4 + e) * 3 + l) * n + t) * 9;
+  int off[9];
+  T w[9];
 #pragma unroll
   for (int s = 0; s < 9; ++s) {
-    const int ii = along_i ? s0 + s : fixed;
-    const int jj = along_i ? fixed : s0 + s;
-    src_off[s] = g.at(k, jj, ii);
-    src_p2[s] = jj * n + ii;
+    const int p2 = a.esrc[row + s];
+    off[s] = (JOFF + p2 / n) * g.pitch + IOFF + p2 % n;
+    w[s] = a.ew[row + s];
   }
-  long long dst;
-  if (e == 0) dst = g.at(k, -1 - l, t);
-  else if (e == 1) dst = g.at(k, n + l, t);
-  else if (e == 2) dst = g.at(k, t, -1 - l);
-  else dst = g.at(k, t, n + l);
-
-  auto scalar = [&](int slot) {
-    const T* src = a.q + g.vol(run, rt.src_face, slot);
-    T acc = T(0);
-#pragma unroll
-    for (int s = 0; s < 9; ++s) acc = fma(w[s], __ldg(src + src_off[s]), acc);
-    a.q[g.vol(run, face, slot) + dst] = acc;
-  };
+  int dst;
+  if (e == 0) dst = (JOFF - 1 - l) * g.pitch + IOFF + t;
+  else if (e == 1) dst = (JOFF + n + l) * g.pitch + IOFF + t;
+  else if (e == 2) dst = (JOFF + t) * g.pitch + IOFF - 1 - l;
+  else dst = (JOFF + t) * g.pitch + IOFF + n + l;
   if (a.mode == 1) {
-    for (int s = 0; s < g.nf; ++s) scalar(s);
+    for (int s = 0; s < g.nf; ++s) {
+      const T* src = a.q + g.vol(run, rt.src_face, s);
+      T* out = a.q + g.vol(run, face, s);
+      for (int k = kb; k < ke; ++k) {
+        const long long kp = (long long)k * g.plane;
+        T acc = T(0);
+#pragma unroll
+        for (int m = 0; m < 9; ++m) acc = fma(w[m], __ldg(src + kp + off[m]), acc);
+        out[kp + dst] = acc;
+      }
+    }
     return;
   }
-  scalar(g.slot[kP]);
-  // vector component: v_xi for W/E receivers, v_eta for S/N receivers
-  const T* vx = a.q + g.vol(run, rt.src_face, g.slot[kVxi]);
-  const T* ve = a.q + g.vol(run, rt.src_face, g.slot[kVeta]);
-  const int kind = rt.src_face < 4 ? 0 : rt.src_face - 3;
-  const long long P2 = (long long)n * n;
-  const T* cv = a.conv + (long long)kind * 4 * P2;
-  T th = T(0), ph = T(0);
+  T gx[9], gy[9];
 #pragma unroll
   for (int s = 0; s < 9; ++s) {
-    const T x = __ldg(vx + src_off[s]), y = __ldg(ve + src_off[s]);
-    const int p2 = src_p2[s];
-    const T tht = fma(cv[p2], x, cv[P2 + p2] * y);
-    const T pht = fma(cv[2 * P2 + p2], x, cv[3 * P2 + p2] * y);
-    th = fma(w[s], tht, th);
-    ph = fma(w[s], pht, ph);
+    gx[s] = a.eg[(row + s) * 2 + 0];
+    gy[s] = a.eg[(row + s) * 2 + 1];
   }
-  const T* rc = a.rot + ((((long long)rt.src_face * 4 + rt.src_edge) * 3 + l) * n + ts) * 2;
-  const int out_slot = (e >= 2) ? g.slot[kVxi] : g.slot[kVeta];
-  a.q[g.vol(run, face, out_slot) + dst] = fma(rc[0], th, rc[1] * ph);
+  const T* sp = a.q + g.vol(run, rt.src_face, g.slot[kP]);
+  const T* sx = a.q + g.vol(run, rt.src_face, g.slot[kVxi]);
+  const T* sy = a.q + g.vol(run, rt.src_face, g.slot[kVeta]);
+  T* op = a.q + g.vol(run, face, g.slot[kP]);
+  T* ov = a.q + g.vol(run, face, (e >= 2) ? g.slot[kVxi] : g.slot[kVeta]);
+#pragma unroll 2
+  for (int k = kb; k < ke; ++k) {
+    const long long kp = (long long)k * g.plane;
+    T ap = T(0), av = T(0);
+#pragma unroll
+    for (int m = 0; m < 9; ++m) {
+      ap = fma(w[m], __ldg(sp + kp + off[m]), ap);
+      av = fma(gx[m], __ldg(sx + kp + off[m]), av);
+      av = fma(gy[m], __ldg(sy + kp + off[m]), av);
+    }
+    op[kp + dst] = ap;
+    ov[kp + dst] = av;
+  }
 }
+
+// radial table rows (must match tables.h)
+enum { rInvR = 0, rFacR, rRho0, rInvRho0, rC2Rho0, rDRho0, rG0Rho0, rRho0G0, rSigma, rCount };
+enum { mD = 0, mXYD, mC, mXYC, mDivX, mDivY, mTX, mTY, mVol, mCount };
 
 // ---------------------------------------------------------------------------------
 // Stage kernel: COMPUTE_RHS (divergence, gradient, background terms) + BC_RHS + SPONGE
 // + the 2N-RK update (timestep.f90:64-69) for one stage, fused.  A CTA owns a TX x TY
-// column tile of one face and marches along k through its chunk.  xi/eta derivatives
-// read shared-memory tiles of plane k with a 3-point halo (from the padded frame at the
-// face edges); the radial derivative reads a 7-plane register window of the thread's own
-// column, shifted as k advances and clamped at the two radial ends where the Tam-Dong
-// one-sided rows apply (derivative.f90:704-754).
+// column tile of one face and marches along k through its chunk of planes.
+//
+// Planes stream in through TMA tile loads into two shared-memory rings, each slot
+// guarded by an mbarrier:
+//   lead ring (kLead slots): the p tile with a 3-point halo and the v_r tile of plane m.
+//     Plane m is needed from iteration m-3 (own values enter the 7-deep radial register
+//     windows of p and v_r) until iteration m (xi/eta derivatives of p).
+//   tile ring (kTile slots): v_xi with its xi halo, v_eta with its eta halo, rho and the
+//     RK registers qw of plane k, needed at iteration k only.
+// Thread 0 refills a slot right after the CTA barrier that closes the iteration using it,
+// so up to kLead-4 lead planes and kTile-1 tile planes are in flight while a plane is
+// computed.  The radial window is clamped at the two ends of the shell, where the
+// Tam-Dong one-sided rows apply (derivative.f90:704-754).
 // MODE 0: RK update, stages 2-5 (reads qw).  MODE 1: RK update, stage 1 (qw = 0).
-// MODE 2: write the raw COMPUTE_RHS into out.  MODE 3: write (grad_xi, grad_eta,
-// grad_r, div) into the v_xi, v_eta, v_r, p slots of out.
+// MODE 2: write the raw COMPUTE_RHS into qout.  MODE 3: write (grad_xi, grad_eta,
+// grad_r, div) into the v_xi, v_eta, v_r, p slots of qout.
+constexpr int kLead = 8;
+constexpr int kTile = 3;
+
 template <typename T>
 struct StageArgs {
-  const T* qin;
+  CUtensorMap mP;           // input buffer, box (TX+8) x (TY+6)
+  CUtensorMap mX;           // input buffer, box (TX+8) x TY
+  CUtensorMap mY;           // input buffer, box TX x (TY+6)
+  CUtensorMap mO;           // input buffer, box TX x TY
+  CUtensorMap mW;           // qw buffer,    box TX x TY
   T* qout;
   T* qw;
   const T* rad;             // [kNumRadial][nr]
   const T* met;             // [kNumMetric][n][n]
   const T* c2;              // optional compact c^2 [face][k][j][i] (run-shared) or nullptr
   const int* active;
+  int* err;
   Geom g;
   T dt, alpha, beta, inv_dxi;
   int kchunk;
 };
 
-// radial table rows (must match tables.h)
-enum { rInvR = 0, rFacR, rRho0, rInvRho0, rC2Rho0, rDRho0, rG0Rho0, rRho0G0, rSigma, rCount };
-enum { mD = 0, mXYD, mC, mXYC, mDivX, mDivY, mTX, mTY, mVol, mCount };
+__host__ __device__ constexpr size_t align128(size_t b) { return (b + 127) / 128 * 128; }
+
+template <typename T, int TX, int TY>
+struct StageLayout {
+  static constexpr int PB = (TX + 8) * (TY + 6), XB = (TX + 8) * TY, YB = TX * (TY + 6), OB = TX * TY;
+  static constexpr size_t P_BYTES = align128(PB * sizeof(T));
+  static constexpr size_t X_BYTES = align128(XB * sizeof(T));
+  static constexpr size_t Y_BYTES = align128(YB * sizeof(T));
+  static constexpr size_t O_BYTES = align128(OB * sizeof(T));
+  static constexpr size_t LEAD = P_BYTES + O_BYTES;                    // p box + v_r
+  static constexpr size_t TILE = X_BYTES + Y_BYTES + 6 * O_BYTES;     // v_xi, v_eta, rho, 5 qw
+  static constexpr size_t BAR = kLead * LEAD + kTile * TILE;
+  static constexpr size_t TOTAL = BAR + (kLead + kTile) * sizeof(uint64_t);
+};
 
 template <typename T, int TX, int TY, int MODE>
-__global__ void __launch_bounds__(TX * TY) stage_kernel(const StageArgs<T> a) {
+__global__ void __launch_bounds__(TX * TY, sizeof(T) == 8 ? 2 : 3) stage_kernel(const __grid_constant__ StageArgs<T> a) {
+  using L = StageLayout<T, TX, TY>;
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L::BAR);
   const Geom& g = a.g;
   const int n = g.n, nr = g.nr;
   const int tiles_x = n / TX;
@@ -195,17 +234,53 @@ __global__ void __launch_bounds__(TX * TY) stage_kernel(const StageArgs<T> a) {
   const int ke = min(nr, kb + a.kchunk);
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
   const int i = i0 + tx, j = j0 + ty;
-
-  __shared__ T sp[TY + 6][TX + 6];
-  __shared__ T sx[TY][TX + 6];
-  __shared__ T sy[TY + 6][TX];
-
   const int sP = g.slot[kP], sX = g.slot[kVxi], sY = g.slot[kVeta], sR = g.slot[kVr], sRho = g.slot[kRho];
-  const T* qP = a.qin + g.vol(run, face, sP);
-  const T* qX = a.qin + g.vol(run, face, sX);
-  const T* qY = a.qin + g.vol(run, face, sY);
-  const T* qR = a.qin + g.vol(run, face, sR);
-  const T* qRho = sRho >= 0 ? a.qin + g.vol(run, face, sRho) : nullptr;
+  const bool has_rho = sRho >= 0 && MODE != 3;
+  const int zbase = (run * 6 + face) * g.nf;   // plane index of (slot s, k) = (zbase + s) * nr + k
+  auto clampk = [nr](int k) { return min(max(k - 3, 0), nr - 7); };
+  const int m_lo = clampk(kb), m_hi = clampk(ke - 1) + 6;
+
+  auto leadP = [&](int m) { return reinterpret_cast<T*>(smem + ((m - m_lo) % kLead) * L::LEAD); };
+  auto leadR = [&](int m) { return reinterpret_cast<T*>(smem + ((m - m_lo) % kLead) * L::LEAD + L::P_BYTES); };
+  auto tileBase = [&](int k) { return smem + kLead * L::LEAD + ((k - kb) % kTile) * L::TILE; };
+  auto tileX = [&](int k) { return reinterpret_cast<T*>(tileBase(k)); };
+  auto tileY = [&](int k) { return reinterpret_cast<T*>(tileBase(k) + L::X_BYTES); };
+  auto tileO = [&](int k, int q) { return reinterpret_cast<T*>(tileBase(k) + L::X_BYTES + L::Y_BYTES + q * L::O_BYTES); };
+  uint64_t* barL = bars;
+  uint64_t* barT = bars + kLead;
+
+  const int xP = IOFF + i0 - 4, yP = JOFF + j0 - 3;   // p / v_xi boxes start 4 columns left
+  const int xO = IOFF + i0, yO = JOFF + j0;
+  auto issue_lead = [&](int m) {
+    uint64_t* b = &barL[(m - m_lo) % kLead];
+    mbar_expect_tx(b, (L::PB + L::OB) * sizeof(T));
+    tma_load_3d(leadP(m), &a.mP, xP, yP, (zbase + sP) * nr + m, b);
+    tma_load_3d(leadR(m), &a.mO, xO, yO, (zbase + sR) * nr + m, b);
+  };
+  auto issue_tile = [&](int k) {
+    uint64_t* b = &barT[(k - kb) % kTile];
+    uint32_t bytes = (L::XB + L::YB) * sizeof(T);
+    if (has_rho) bytes += L::OB * sizeof(T);
+    if (MODE == 0) bytes += g.nf * L::OB * sizeof(T);
+    mbar_expect_tx(b, bytes);
+    tma_load_3d(tileX(k), &a.mX, xP, yO, (zbase + sX) * nr + k, b);
+    tma_load_3d(tileY(k), &a.mY, xO, yP, (zbase + sY) * nr + k, b);
+    if (has_rho) tma_load_3d(tileO(k, 0), &a.mO, xO, yO, (zbase + sRho) * nr + k, b);
+    if (MODE == 0)
+      for (int s = 0; s < g.nf; ++s) tma_load_3d(tileO(k, 1 + s), &a.mW, xO, yO, (zbase + s) * nr + k, b);
+  };
+
+  if (tid == 0) {
+    for (int q = 0; q < kLead + kTile; ++q) mbar_init(&bars[q], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  int m_issued = m_lo;
+  if (tid == 0) {
+    tma_prefetch_desc(&a.mP);
+    for (; m_issued <= min(m_lo + kLead - 1, m_hi); ++m_issued) issue_lead(m_issued);
+    for (int k = kb; k < min(kb + kTile, ke); ++k) issue_tile(k);
+  }
 
   const long long P2 = (long long)n * n;
   const int p2 = j * n + i;
@@ -214,54 +289,38 @@ __global__ void __launch_bounds__(TX * TY) stage_kernel(const StageArgs<T> a) {
   const T m_DivX = a.met[mDivX * P2 + p2], m_DivY = a.met[mDivY * P2 + p2];
   const T m_TX = a.met[mTX * P2 + p2], m_TY = a.met[mTY * P2 + p2];
   const T c1 = Coef<T>::drp(1), c2 = Coef<T>::drp(2), c3 = Coef<T>::drp(3);
-
   const long long own = g.at(0, j, i);
-  auto clampk = [nr](int k) { return min(max(k - 3, 0), nr - 7); };
-  T pw[7], vw[7];
-  int ks = clampk(kb);
-#pragma unroll
-  for (int s = 0; s < 7; ++s) {
-    pw[s] = qP[(long long)(ks + s) * g.plane + own];
-    vw[s] = qR[(long long)(ks + s) * g.plane + own];
-  }
+  constexpr int PW = TX + 8;
+  const int pc = (ty + 3) * PW + tx + 4;              // own point inside the p box
 
+  T pw[7], vw[7];
+#pragma unroll
+  for (int s = 0; s < 7; ++s) { pw[s] = T(0); vw[s] = T(0); }
+  int mq = m_lo;
+  bool ok = true;
   for (int k = kb; k < ke; ++k) {
-    const int ksn = clampk(k);
-    if (ksn != ks) {
+    const int ks = clampk(k);
+    for (; mq <= ks + 6; ++mq) {
+      ok &= mbar_wait(&barL[(mq - m_lo) % kLead], ((mq - m_lo) / kLead) & 1, a.err, 1);
 #pragma unroll
       for (int s = 0; s < 6; ++s) { pw[s] = pw[s + 1]; vw[s] = vw[s + 1]; }
-      ks = ksn;
-      pw[6] = qP[(long long)(ks + 6) * g.plane + own];
-      vw[6] = qR[(long long)(ks + 6) * g.plane + own];
+      pw[6] = leadP(mq)[pc];
+      vw[6] = leadR(mq)[ty * TX + tx];
     }
-    const long long kp = (long long)k * g.plane;
-    __syncthreads();
-    for (int idx = tid; idx < (TY + 6) * (TX + 6); idx += TX * TY) {
-      const int r = idx / (TX + 6), c = idx % (TX + 6);
-      sp[r][c] = qP[kp + g.at(0, j0 - 3 + r, i0 - 3 + c)];
-    }
-    for (int idx = tid; idx < TY * (TX + 6); idx += TX * TY) {
-      const int r = idx / (TX + 6), c = idx % (TX + 6);
-      sx[r][c] = qX[kp + g.at(0, j0 + r, i0 - 3 + c)];
-    }
-    for (int idx = tid; idx < (TY + 6) * TX; idx += TX * TY) {
-      const int r = idx / TX, c = idx % TX;
-      sy[r][c] = qY[kp + g.at(0, j0 - 3 + r, i0 + c)];
-    }
-    __syncthreads();
-
-    const T dpx = a.inv_dxi * (c1 * (sp[ty + 3][tx + 4] - sp[ty + 3][tx + 2]) +
-                               c2 * (sp[ty + 3][tx + 5] - sp[ty + 3][tx + 1]) +
-                               c3 * (sp[ty + 3][tx + 6] - sp[ty + 3][tx]));
-    const T dpy = a.inv_dxi * (c1 * (sp[ty + 4][tx + 3] - sp[ty + 2][tx + 3]) +
-                               c2 * (sp[ty + 5][tx + 3] - sp[ty + 1][tx + 3]) +
-                               c3 * (sp[ty + 6][tx + 3] - sp[ty][tx + 3]));
-    const T dvx = a.inv_dxi * (c1 * (sx[ty][tx + 4] - sx[ty][tx + 2]) +
-                               c2 * (sx[ty][tx + 5] - sx[ty][tx + 1]) +
-                               c3 * (sx[ty][tx + 6] - sx[ty][tx]));
-    const T dvy = a.inv_dxi * (c1 * (sy[ty + 4][tx] - sy[ty + 2][tx]) +
-                               c2 * (sy[ty + 5][tx] - sy[ty + 1][tx]) +
-                               c3 * (sy[ty + 6][tx] - sy[ty][tx]));
+    ok &= mbar_wait(&barT[(k - kb) % kTile], ((k - kb) / kTile) & 1, a.err, 2);
+    const T* sp = leadP(k);
+    const T* sx = tileX(k);
+    const T* sy = tileY(k);
+    const T dpx = a.inv_dxi * (c1 * (sp[pc + 1] - sp[pc - 1]) + c2 * (sp[pc + 2] - sp[pc - 2]) +
+                               c3 * (sp[pc + 3] - sp[pc - 3]));
+    const T dpy = a.inv_dxi * (c1 * (sp[pc + PW] - sp[pc - PW]) + c2 * (sp[pc + 2 * PW] - sp[pc - 2 * PW]) +
+                               c3 * (sp[pc + 3 * PW] - sp[pc - 3 * PW]));
+    const int xc = ty * PW + tx + 4;
+    const T dvx = a.inv_dxi * (c1 * (sx[xc + 1] - sx[xc - 1]) + c2 * (sx[xc + 2] - sx[xc - 2]) +
+                               c3 * (sx[xc + 3] - sx[xc - 3]));
+    const int yc = (ty + 3) * TX + tx;
+    const T dvy = a.inv_dxi * (c1 * (sy[yc + TX] - sy[yc - TX]) + c2 * (sy[yc + 2 * TX] - sy[yc - 2 * TX]) +
+                               c3 * (sy[yc + 3 * TX] - sy[yc - 3 * TX]));
     const T facr = a.rad[rFacR * nr + k];
     T dpr, dvr;
     if (k >= 3 && k <= nr - 4) {
@@ -269,73 +328,81 @@ __global__ void __launch_bounds__(TX * TY) stage_kernel(const StageArgs<T> a) {
       dvr = facr * (c1 * (vw[4] - vw[2]) + c2 * (vw[5] - vw[1]) + c3 * (vw[6] - vw[0]));
     } else {
       const bool lo = k < 3;
-      const int row = lo ? k : nr - 1 - k;
-      T sp_ = T(0), sv_ = T(0);
+      const int brow = lo ? k : nr - 1 - k;
+      T a_ = T(0), b_ = T(0);
 #pragma unroll
       for (int s = 0; s < 7; ++s) {
-        const T b = Coef<T>::bdy(row, lo ? s : 6 - s);
-        sp_ = fma(b, pw[s], sp_);
-        sv_ = fma(b, vw[s], sv_);
+        const T b = Coef<T>::bdy(brow, lo ? s : 6 - s);
+        a_ = fma(b, pw[s], a_);
+        b_ = fma(b, vw[s], b_);
       }
-      dpr = lo ? facr * sp_ : -facr * sp_;
-      dvr = lo ? facr * sv_ : -facr * sv_;
+      dpr = lo ? facr * a_ : -facr * a_;
+      dvr = lo ? facr * b_ : -facr * b_;
     }
-    const int off = k - ks;
+    const int offk = k - ks;
     T vr = vw[0];
 #pragma unroll
-    for (int s = 1; s < 7; ++s) vr = (off == s) ? vw[s] : vr;
-    const T p = sp[ty + 3][tx + 3];
-    const T vxi = sx[ty][tx + 3];
-    const T veta = sy[ty + 3][tx];
-
+    for (int s = 1; s < 7; ++s) vr = (offk == s) ? vw[s] : vr;
+    const T p = sp[pc];
+    const T vxi = sx[xc];
+    const T veta = sy[yc];
     const T invr = a.rad[rInvR * nr + k];
     const T gxi = invr * (m_D * dpx + m_XYD * dpy);
     const T geta = invr * (m_C * dpy + m_XYC * dpx);
     const T div = invr * (m_DivX * dvx + m_DivY * dvy - m_TX * vxi - m_TY * veta) + dvr + T(2) * vr * invr;
-    const long long pt = kp + own;
-
+    const long long pt = (long long)k * g.plane + own;
     if (MODE == 3) {
       a.qout[g.vol(run, face, sX) + pt] = gxi;
       a.qout[g.vol(run, face, sY) + pt] = geta;
       a.qout[g.vol(run, face, sR) + pt] = dpr;
       a.qout[g.vol(run, face, sP) + pt] = div;
-      continue;
+    } else {
+      const T rho0 = a.rad[rRho0 * nr + k], inv_rho0 = a.rad[rInvRho0 * nr + k];
+      T c2rho0 = a.rad[rC2Rho0 * nr + k];
+      if (a.c2) c2rho0 = a.c2[((long long)face * nr + k) * P2 + p2] * rho0;
+      const int oc = ty * TX + tx;
+      const T rho = has_rho ? tileO(k, 0)[oc] : T(0);
+      T r_rho = -rho0 * div - vr * a.rad[rDRho0 * nr + k];
+      T r_vx = -gxi * inv_rho0;
+      T r_ve = -geta * inv_rho0;
+      T r_vr = -dpr * inv_rho0 - rho * a.rad[rG0Rho0 * nr + k];
+      T r_p = -c2rho0 * div + a.rad[rRho0G0 * nr + k] * vr;
+      if (MODE == 2) {
+        if (has_rho) a.qout[g.vol(run, face, sRho) + pt] = r_rho;
+        a.qout[g.vol(run, face, sX) + pt] = r_vx;
+        a.qout[g.vol(run, face, sY) + pt] = r_ve;
+        a.qout[g.vol(run, face, sR) + pt] = r_vr;
+        a.qout[g.vol(run, face, sP) + pt] = r_p;
+      } else {
+        // BC_RHS (bc_acoustic_wave.f90:432-452) then SPONGE (sponge.f90:502-504)
+        if (k == 0 || k == nr - 1) { r_rho = r_vx = r_ve = r_vr = r_p = T(0); }
+        const T sig = a.rad[rSigma * nr + k];
+        r_rho -= sig * rho;
+        r_vr -= sig * vr;
+        r_p -= sig * p;
+        // qw = alpha qw + dt rhs ; q = q + beta qw   (timestep.f90:68-69)
+        auto update = [&](int s, T q, T r) {
+          const T w = (MODE == 1) ? a.dt * r : fma(a.alpha, tileO(k, 1 + s)[oc], a.dt * r);
+          a.qw[g.vol(run, face, s) + pt] = w;
+          a.qout[g.vol(run, face, s) + pt] = fma(a.beta, w, q);
+        };
+        if (has_rho) update(sRho, rho, r_rho);
+        update(sX, vxi, r_vx);
+        update(sY, veta, r_ve);
+        update(sR, vr, r_vr);
+        update(sP, p, r_p);
+      }
     }
-    const T rho0 = a.rad[rRho0 * nr + k], inv_rho0 = a.rad[rInvRho0 * nr + k];
-    T c2rho0 = a.rad[rC2Rho0 * nr + k];
-    if (a.c2) c2rho0 = a.c2[((long long)face * nr + k) * P2 + p2] * rho0;
-    const T rho = qRho ? qRho[pt] : T(0);
-    T r_rho = -rho0 * div - vr * a.rad[rDRho0 * nr + k];
-    T r_vx = -gxi * inv_rho0;
-    T r_ve = -geta * inv_rho0;
-    T r_vr = -dpr * inv_rho0 - rho * a.rad[rG0Rho0 * nr + k];
-    T r_p = -c2rho0 * div + a.rad[rRho0G0 * nr + k] * vr;
-    if (MODE == 2) {
-      if (qRho) a.qout[g.vol(run, face, sRho) + pt] = r_rho;
-      a.qout[g.vol(run, face, sX) + pt] = r_vx;
-      a.qout[g.vol(run, face, sY) + pt] = r_ve;
-      a.qout[g.vol(run, face, sR) + pt] = r_vr;
-      a.qout[g.vol(run, face, sP) + pt] = r_p;
-      continue;
+    // every thread is done with lead plane k and tile plane k: refill their slots
+    if (__syncthreads_or(!ok)) break;
+    if (tid == 0) {
+      if (k + kTile < ke) issue_tile(k + kTile);
+      for (; m_issued <= min(k + kLead, m_hi); ++m_issued) issue_lead(m_issued);
     }
-    // BC_RHS (bc_acoustic_wave.f90:432-452) then SPONGE (sponge.f90:502-504)
-    if (k == 0 || k == nr - 1) { r_rho = r_vx = r_ve = r_vr = r_p = T(0); }
-    const T sig = a.rad[rSigma * nr + k];
-    r_rho -= sig * rho;
-    r_vr -= sig * vr;
-    r_p -= sig * p;
-    // qw = alpha qw + dt rhs ; q = q + beta qw   (timestep.f90:68-69)
-    auto update = [&](int s, T q, T r) {
-      T* W = a.qw + g.vol(run, face, s) + pt;
-      const T w = (MODE == 1) ? a.dt * r : fma(a.alpha, *W, a.dt * r);
-      *W = w;
-      a.qout[g.vol(run, face, s) + pt] = fma(a.beta, w, q);
-    };
-    if (qRho) update(sRho, rho, r_rho);
-    update(sX, vxi, r_vx);
-    update(sY, veta, r_ve);
-    update(sR, vr, r_vr);
-    update(sP, p, r_p);
+  }
+  if (!ok && tid == 0) {
+    // a wait gave up: give copies still in flight a bounded time to land before exit
+    for (int q = 0; q < 1000; ++q) __nanosleep(1000);
   }
 }
 
@@ -344,17 +411,33 @@ __global__ void __launch_bounds__(TX * TY) stage_kernel(const StageArgs<T> a) {
 // q halos), eta filter of that (rows outside the face take the UNFILTERED q halo,
 // filter.f90:43), 11-point radial filter of the result; the 5 end planes at each radial
 // end become 0 (filter.f90:726-775).  A CTA owns a TX x TY column tile of one face and
-// one field and marches through every k with an 11-deep register queue.
+// one field and streams every plane through a kFilt-deep TMA ring, keeping the last 11
+// eta-filtered values of its column in registers.
+constexpr int kFiltRing = 4;
+
 template <typename T>
 struct FilterArgs {
-  const T* qin;
+  CUtensorMap mP;           // input buffer, box (TX+8) x (TY+6)
   T* qout;
   const int* active;
+  int* err;
   Geom g;
 };
 
 template <typename T, int TX, int TY>
-__global__ void __launch_bounds__(TX * TY) filter_kernel(const FilterArgs<T> a) {
+struct FilterLayout {
+  static constexpr int PB = (TX + 8) * (TY + 6), SB = (TY + 6) * TX;
+  static constexpr size_t P_BYTES = align128(PB * sizeof(T));
+  static constexpr size_t S_BYTES = align128(SB * sizeof(T));
+  static constexpr size_t BAR = kFiltRing * P_BYTES + 2 * S_BYTES;
+  static constexpr size_t TOTAL = BAR + kFiltRing * sizeof(uint64_t);
+};
+
+template <typename T, int TX, int TY>
+__global__ void __launch_bounds__(TX * TY) filter_kernel(const __grid_constant__ FilterArgs<T> a) {
+  using L = FilterLayout<T, TX, TY>;
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L::BAR);
   const Geom& g = a.g;
   const int n = g.n, nr = g.nr;
   const int tiles_x = n / TX;
@@ -364,37 +447,46 @@ __global__ void __launch_bounds__(TX * TY) filter_kernel(const FilterArgs<T> a) 
   if (a.active && !a.active[run]) return;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
   const int i = i0 + tx, j = j0 + ty;
-  __shared__ T sq[TY + 6][TX + 6];
-  __shared__ T st[TY + 6][TX];
-  const T* q = a.qin + g.vol(run, face, s);
+  constexpr int PW = TX + 8;
+  auto box = [&](int k) { return reinterpret_cast<const T*>(smem + (k % kFiltRing) * L::P_BYTES); };
+  auto st = [&](int k) { return reinterpret_cast<T*>(smem + kFiltRing * L::P_BYTES + (k & 1) * L::S_BYTES); };
+  const int z0 = ((run * 6 + face) * g.nf + s) * nr;
+  const int xP = IOFF + i0 - 4, yP = JOFF + j0 - 3;
+  auto issue = [&](int k) {
+    uint64_t* b = &bars[k % kFiltRing];
+    mbar_expect_tx(b, L::PB * sizeof(T));
+    tma_load_3d(smem + (k % kFiltRing) * L::P_BYTES, &a.mP, xP, yP, z0 + k, b);
+  };
+  if (tid == 0) {
+    for (int q = 0; q < kFiltRing; ++q) mbar_init(&bars[q], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  if (tid == 0)
+    for (int k = 0; k < min(kFiltRing, nr); ++k) issue(k);
   T* out = a.qout + g.vol(run, face, s);
   const long long own = g.at(0, j, i);
   const T f0 = Coef<T>::filt(0), f1 = Coef<T>::filt(1), f2 = Coef<T>::filt(2), f3 = Coef<T>::filt(3);
   T tq[11];
 #pragma unroll
   for (int m = 0; m < 11; ++m) tq[m] = T(0);
+  bool ok = true;
   for (int k = 0; k < nr; ++k) {
-    const long long kp = (long long)k * g.plane;
-    __syncthreads();
-    for (int idx = tid; idx < (TY + 6) * (TX + 6); idx += TX * TY) {
-      const int r = idx / (TX + 6), c = idx % (TX + 6);
-      sq[r][c] = q[kp + g.at(0, j0 - 3 + r, i0 - 3 + c)];
-    }
-    __syncthreads();
+    ok &= mbar_wait(&bars[k % kFiltRing], (k / kFiltRing) & 1, a.err, 3);
+    const T* bx = box(k);
+    T* t1 = st(k);
     for (int r = ty; r < TY + 6; r += TY) {
       const int jr = j0 - 3 + r;
+      const T* row = bx + r * PW + tx + 4;
       T v;
-      if (jr < 0 || jr >= n) {
-        v = sq[r][tx + 3];
-      } else {
-        v = f0 * sq[r][tx + 3] + f1 * (sq[r][tx + 2] + sq[r][tx + 4]) +
-            f2 * (sq[r][tx + 1] + sq[r][tx + 5]) + f3 * (sq[r][tx] + sq[r][tx + 6]);
-      }
-      st[r][tx] = v;
+      if (jr < 0 || jr >= n) v = row[0];
+      else v = f0 * row[0] + f1 * (row[-1] + row[1]) + f2 * (row[-2] + row[2]) + f3 * (row[-3] + row[3]);
+      t1[r * TX + tx] = v;
     }
-    __syncthreads();
-    const T t2 = f0 * st[ty + 3][tx] + f1 * (st[ty + 2][tx] + st[ty + 4][tx]) +
-                 f2 * (st[ty + 1][tx] + st[ty + 5][tx]) + f3 * (st[ty][tx] + st[ty + 6][tx]);
+    if (__syncthreads_or(!ok)) break;
+    if (tid == 0 && k + kFiltRing < nr) issue(k + kFiltRing);
+    const T* c = t1 + (ty + 3) * TX + tx;
+    const T t2 = f0 * c[0] + f1 * (c[-TX] + c[TX]) + f2 * (c[-2 * TX] + c[2 * TX]) + f3 * (c[-3 * TX] + c[3 * TX]);
 #pragma unroll
     for (int m = 0; m < 10; ++m) tq[m] = tq[m + 1];
     tq[10] = t2;
@@ -404,8 +496,10 @@ __global__ void __launch_bounds__(TX * TY) filter_kernel(const FilterArgs<T> a) 
       for (int m = 1; m <= 5; ++m) v += Coef<T>::filtr(m) * (tq[5 - m] + tq[5 + m]);
       out[(long long)(k - 5) * g.plane + own] = v;
     }
-    if (k < 5 || k >= nr - 5) out[kp + own] = T(0);
+    if (k < 5 || k >= nr - 5) out[(long long)k * g.plane + own] = T(0);
   }
+  if (!ok && tid == 0)
+    for (int q = 0; q < 1000; ++q) __nanosleep(1000);
 }
 
 // ---------------------------------------------------------------------------------

@@ -1,5 +1,7 @@
 // solar_gpu.cu -- context management and the C-ABI of include/solar_gpu.h.
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cmath>
@@ -39,10 +41,10 @@ struct DevTables {
   void* rad = nullptr;     // T [kNumRadial][nr]
   void* met = nullptr;     // T [kNumMetric][n][n]
   void* conv = nullptr;    // T [3][4][n][n]
-  void* w9 = nullptr;      // T [3][n][9]
-  void* rot = nullptr;     // T [6][4][3][n][2]
+  void* ew = nullptr;      // T [6][4][3][n][9]     folded edge weights (scalar)
+  void* eg = nullptr;      // T [6][4][3][n][9][2]  folded edge weights (vector)
+  int* esrc = nullptr;     // [6][4][3][n][9]
   void* c2 = nullptr;      // T [6][nr][n][n] optional
-  int* s0 = nullptr;       // [3][n]
   double* rad64 = nullptr; // FP64 copies for diagnostics
   double* vol2 = nullptr;  // [n][n]
   double* drw = nullptr;   // [nr]
@@ -72,8 +74,9 @@ struct solar_ctx {
   int* active = nullptr;       // batched runs
   int* target = nullptr;
   int* done = nullptr;
+  int* err = nullptr;          // device error word (bounded waits that gave up)
   DevTables dt;
-  int tile_x = 32, tile_y = 8, kchunk = 0;
+  int tile_x = 32, tile_y = 8, kchunk = 0, edge_kchunk = 16;
   cudaGraphExec_t step_graph = nullptr;
   cudaGraphExec_t batch_graph = nullptr;
   cudaEvent_t ev[8] = {};
@@ -94,9 +97,8 @@ static int upload_tables(solar_ctx* c) {
   int rc;
   if ((rc = upload<T>(&c->dt.rad, c->ht.radial))) return rc;
   if ((rc = upload<T>(&c->dt.met, c->ht.metric))) return rc;
-  if ((rc = upload<T>(&c->dt.conv, c->ht.conv))) return rc;
-  if ((rc = upload<T>(&c->dt.w9, c->ht.w9))) return rc;
-  if ((rc = upload<T>(&c->dt.rot, c->ht.rot))) return rc;
+  if ((rc = upload<T>(&c->dt.ew, c->ht.ew))) return rc;
+  if ((rc = upload<T>(&c->dt.eg, c->ht.eg))) return rc;
   return SOLAR_OK;
 }
 
@@ -124,81 +126,140 @@ static int upload_constants() {
 }
 
 // ---------------------------------------------------------------- launches
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no -lcuda needed).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// 3-D view of a whole buffer: x = padded column, y = padded row, z = plane index
+// ((run*6 + face)*nf + slot)*nr + k; box bx x by x 1.
+static bool make_map(const solar_ctx* c, const void* base, int bx, int by, CUtensorMap* m) {
+  auto enc = tensor_map_encoder();
+  if (!enc) return false;
+  const Geom& g = c->g;
+  cuuint64_t dims[3] = {(cuuint64_t)g.pitch, (cuuint64_t)g.rows, (cuuint64_t)g.nruns * 6 * g.nf * g.nr};
+  cuuint64_t strides[2] = {(cuuint64_t)g.pitch * c->esize, (cuuint64_t)g.plane * c->esize};
+  cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = enc(m, c->fp32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
+                   const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
 template <typename T>
-static void launch_edge(solar_ctx* c, void* buf, int mode, const int* active) {
+static int launch_edge(solar_ctx* c, void* buf, int mode, const int* active) {
   EdgeArgs<T> a;
   a.q = (T*)buf;
-  a.w9 = (const T*)c->dt.w9;
-  a.s0 = c->dt.s0;
-  a.conv = (const T*)c->dt.conv;
-  a.rot = (const T*)c->dt.rot;
+  a.ew = (const T*)c->dt.ew;
+  a.eg = (const T*)c->dt.eg;
+  a.esrc = c->dt.esrc;
   a.active = active;
   a.g = c->g;
   a.mode = mode;
+  a.kchunk = c->edge_kchunk;
   dim3 block(64, 3);
-  dim3 grid((c->g.n + 63) / 64, c->g.nr, c->g.nruns * 24);
+  dim3 grid((c->g.n + 63) / 64, (c->g.nr + a.kchunk - 1) / a.kchunk, c->g.nruns * 24);
   edge_kernel<T><<<grid, block, 0, c->stream>>>(a);
+  return SOLAR_OK;
+}
+
+template <typename T, int TX, int TY, int MODE>
+static int launch_stage_t(solar_ctx* c, StageArgs<T>& a, const void* qin) {
+  using L = StageLayout<T, TX, TY>;
+  if (!make_map(c, qin, TX + 8, TY + 6, &a.mP) || !make_map(c, qin, TX + 8, TY, &a.mX) ||
+      !make_map(c, qin, TX, TY + 6, &a.mY) || !make_map(c, qin, TX, TY, &a.mO) ||
+      !make_map(c, c->W, TX, TY, &a.mW))
+    return fail(SOLAR_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+  static bool attr_set = false;
+  if (!attr_set) {
+    CK(cudaFuncSetAttribute(stage_kernel<T, TX, TY, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::TOTAL));
+    attr_set = true;
+  }
+  const int nchunks = (c->g.nr + a.kchunk - 1) / a.kchunk;
+  dim3 grid((c->g.n / TX) * (c->g.n / TY), nchunks, c->g.nruns * 6);
+  stage_kernel<T, TX, TY, MODE><<<grid, dim3(TX, TY), L::TOTAL, c->stream>>>(a);
+  return SOLAR_OK;
 }
 
 template <typename T, int TX, int TY>
-static void launch_stage_t(solar_ctx* c, const StageArgs<T>& a, int mode) {
-  const int nchunks = (c->g.nr + a.kchunk - 1) / a.kchunk;
-  dim3 grid((c->g.n / TX) * (c->g.n / TY), nchunks, c->g.nruns * 6);
-  dim3 block(TX, TY);
+static int launch_stage_mode(solar_ctx* c, StageArgs<T>& a, const void* qin, int mode) {
   switch (mode) {
-    case 0: stage_kernel<T, TX, TY, 0><<<grid, block, 0, c->stream>>>(a); break;
-    case 1: stage_kernel<T, TX, TY, 1><<<grid, block, 0, c->stream>>>(a); break;
-    case 2: stage_kernel<T, TX, TY, 2><<<grid, block, 0, c->stream>>>(a); break;
-    default: stage_kernel<T, TX, TY, 3><<<grid, block, 0, c->stream>>>(a); break;
+    case 0: return launch_stage_t<T, TX, TY, 0>(c, a, qin);
+    case 1: return launch_stage_t<T, TX, TY, 1>(c, a, qin);
+    case 2: return launch_stage_t<T, TX, TY, 2>(c, a, qin);
+    default: return launch_stage_t<T, TX, TY, 3>(c, a, qin);
   }
 }
 
 template <typename T>
-static void launch_stage(solar_ctx* c, const void* qin, void* qout, int mode, int stage,
-                         const int* active) {
+static int launch_stage(solar_ctx* c, const void* qin, void* qout, int mode, int stage,
+                        const int* active) {
   StageArgs<T> a;
-  a.qin = (const T*)qin;
   a.qout = (T*)qout;
   a.qw = (T*)c->W;
   a.rad = (const T*)c->dt.rad;
   a.met = (const T*)c->dt.met;
   a.c2 = (const T*)c->dt.c2;
   a.active = active;
+  a.err = c->err;
   a.g = c->g;
   a.dt = (T)c->desc.dt;
   a.alpha = (T)kAlpha[stage];
   a.beta = (T)kBeta[stage];
   a.inv_dxi = (T)(1.0 / c->ht.dxi);
   a.kchunk = c->kchunk;
-  if (c->tile_x == 16 && c->tile_y == 8) launch_stage_t<T, 16, 8>(c, a, mode);
-  else if (c->tile_x == 32 && c->tile_y == 4) launch_stage_t<T, 32, 4>(c, a, mode);
-  else if (c->tile_x == 32 && c->tile_y == 16) launch_stage_t<T, 32, 16>(c, a, mode);
-  else if (c->tile_x == 16 && c->tile_y == 16) launch_stage_t<T, 16, 16>(c, a, mode);
-  else launch_stage_t<T, 32, 8>(c, a, mode);
+  if (mode >= 2) {  // operator-level calls use the default tile
+    if (c->g.n % 32 == 0) return launch_stage_mode<T, 32, 8>(c, a, qin, mode);
+    return launch_stage_mode<T, 16, 8>(c, a, qin, mode);
+  }
+  if (c->tile_x == 16 && c->tile_y == 8) return launch_stage_mode<T, 16, 8>(c, a, qin, mode);
+  if (c->tile_x == 32 && c->tile_y == 4) return launch_stage_mode<T, 32, 4>(c, a, qin, mode);
+  if (c->tile_x == 64 && c->tile_y == 4) return launch_stage_mode<T, 64, 4>(c, a, qin, mode);
+  if (c->tile_x == 16 && c->tile_y == 16) return launch_stage_mode<T, 16, 16>(c, a, qin, mode);
+  return launch_stage_mode<T, 32, 8>(c, a, qin, mode);
+}
+
+template <typename T, int TX, int TY>
+static int launch_filter_t(solar_ctx* c, const void* qin, void* qout, const int* active) {
+  using L = FilterLayout<T, TX, TY>;
+  FilterArgs<T> a;
+  if (!make_map(c, qin, TX + 8, TY + 6, &a.mP)) return fail(SOLAR_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+  a.qout = (T*)qout;
+  a.active = active;
+  a.err = c->err;
+  a.g = c->g;
+  static bool attr_set = false;
+  if (!attr_set) {
+    CK(cudaFuncSetAttribute(filter_kernel<T, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::TOTAL));
+    attr_set = true;
+  }
+  dim3 grid((c->g.n / TX) * (c->g.n / TY), c->g.nf, c->g.nruns * 6);
+  filter_kernel<T, TX, TY><<<grid, dim3(TX, TY), L::TOTAL, c->stream>>>(a);
+  return SOLAR_OK;
 }
 
 template <typename T>
-static void launch_filter(solar_ctx* c, const void* qin, void* qout, const int* active) {
-  FilterArgs<T> a;
-  a.qin = (const T*)qin;
-  a.qout = (T*)qout;
-  a.active = active;
-  a.g = c->g;
-  if (c->g.n % 32 == 0) {
-    dim3 grid((c->g.n / 32) * (c->g.n / 8), c->g.nf, c->g.nruns * 6);
-    filter_kernel<T, 32, 8><<<grid, dim3(32, 8), 0, c->stream>>>(a);
-  } else {
-    dim3 grid((c->g.n / 16) * (c->g.n / 8), c->g.nf, c->g.nruns * 6);
-    filter_kernel<T, 16, 8><<<grid, dim3(16, 8), 0, c->stream>>>(a);
-  }
+static int launch_filter(solar_ctx* c, const void* qin, void* qout, const int* active) {
+  if (c->g.n % 32 == 0) return launch_filter_t<T, 32, 8>(c, qin, qout, active);
+  return launch_filter_t<T, 16, 8>(c, qin, qout, active);
 }
 
 // One full time step (timestep.f90:61-82) on every run.  With ev != nullptr each kernel
 // is bracketed by events: ev_pairs[kind] accumulates into times[kind].
 template <typename T>
-static void enqueue_step(solar_ctx* c, const int* active, std::vector<cudaEvent_t>* evs) {
+static int enqueue_step(solar_ctx* c, const int* active, std::vector<cudaEvent_t>* evs) {
   void* bufs[2] = {c->A, c->B};
-  int cur = 0;
+  int cur = 0, rc;
   auto mark = [&]() {
     if (!evs) return;
     cudaEvent_t e;
@@ -208,30 +269,44 @@ static void enqueue_step(solar_ctx* c, const int* active, std::vector<cudaEvent_
   };
   for (int s = 0; s < 5; ++s) {
     mark();
-    launch_edge<T>(c, bufs[cur], 0, active);
+    if ((rc = launch_edge<T>(c, bufs[cur], 0, active))) return rc;
     mark();
-    launch_stage<T>(c, bufs[cur], bufs[cur ^ 1], s == 0 ? 1 : 0, s, active);
+    if ((rc = launch_stage<T>(c, bufs[cur], bufs[cur ^ 1], s == 0 ? 1 : 0, s, active))) return rc;
     mark();
     cur ^= 1;
   }
   mark();
-  launch_edge<T>(c, bufs[cur], 1, active);
+  if ((rc = launch_edge<T>(c, bufs[cur], 1, active))) return rc;
   mark();
-  launch_filter<T>(c, bufs[cur], bufs[cur ^ 1], active);
+  if ((rc = launch_filter<T>(c, bufs[cur], bufs[cur ^ 1], active))) return rc;
   mark();
+  return SOLAR_OK;
 }
 
-static void enqueue_step_any(solar_ctx* c, const int* active, std::vector<cudaEvent_t>* evs) {
-  if (c->fp32) enqueue_step<float>(c, active, evs);
-  else enqueue_step<double>(c, active, evs);
+static int enqueue_step_any(solar_ctx* c, const int* active, std::vector<cudaEvent_t>* evs) {
+  return c->fp32 ? enqueue_step<float>(c, active, evs) : enqueue_step<double>(c, active, evs);
+}
+
+// Device error word: set by a kernel whose bounded wait gave up.
+static int check_device_error(solar_ctx* c) {
+  int h = 0;
+  CK(cudaMemcpyAsync(&h, c->err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (h) {
+    cudaMemsetAsync(c->err, 0, sizeof(int), c->stream);
+    return fail(SOLAR_ERR_TIMEOUT, "a device wait gave up (code %d)", h);
+  }
+  return SOLAR_OK;
 }
 
 static int capture_step_graph(solar_ctx* c) {
   if (c->step_graph) return SOLAR_OK;
   cudaGraph_t graph;
   CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-  enqueue_step_any(c, nullptr, nullptr);
-  CK(cudaStreamEndCapture(c->stream, &graph));
+  int rc = enqueue_step_any(c, nullptr, nullptr);
+  cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
+  if (rc) return rc;
+  CK(ce);
   CK(cudaGraphInstantiate(&c->step_graph, graph, 0));
   CK(cudaGraphDestroy(graph));
   return SOLAR_OK;
@@ -243,9 +318,11 @@ static int capture_batch_graph(solar_ctx* c) {
   cudaGraph_t graph;
   CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
   batch_tick_kernel<<<(R + 127) / 128, 128, 0, c->stream>>>(c->target, c->done, c->active, R);
-  enqueue_step_any(c, c->active, nullptr);
+  int rc = enqueue_step_any(c, c->active, nullptr);
   batch_tock_kernel<<<(R + 127) / 128, 128, 0, c->stream>>>(c->active, c->done, R);
-  CK(cudaStreamEndCapture(c->stream, &graph));
+  cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
+  if (rc) return rc;
+  CK(ce);
   CK(cudaGraphInstantiate(&c->batch_graph, graph, 0));
   CK(cudaGraphDestroy(graph));
   return SOLAR_OK;
@@ -360,7 +437,7 @@ int solar_gpu_finalize(solar_ctx* c) {
   if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
   if (c->batch_graph) cudaGraphExecDestroy(c->batch_graph);
   void* ptrs[] = {c->A, c->B, c->W, c->stage64, c->part, c->red_out, c->active, c->target, c->done,
-                  c->dt.rad, c->dt.met, c->dt.conv, c->dt.w9, c->dt.rot, c->dt.c2, c->dt.s0,
+                  c->err, c->dt.rad, c->dt.met, c->dt.ew, c->dt.eg, c->dt.esrc, c->dt.c2,
                   c->dt.rad64, c->dt.vol2, c->dt.drw, c->dt.c2_64, c->dt.tanx, c->dt.gr};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -398,7 +475,7 @@ int solar_gpu_init(const solar_desc* d, solar_ctx** out) {
   g.pitch = d->nx + 2 * IOFF;
   g.rows = d->nx + 2 * JOFF;
   g.plane = (long long)g.pitch * g.rows;
-  g.vs = ((g.plane * g.nr + 63) / 64) * 64;
+  g.vs = g.plane * g.nr;   // volumes back to back: the whole buffer is one 3-D array of planes
   g.nruns = d->nruns;
   if (g.nf == 5) { for (int f = 0; f < 5; ++f) g.slot[f] = f; }
   else { g.slot[kRho] = -1; g.slot[kVxi] = 0; g.slot[kVeta] = 1; g.slot[kVr] = 2; g.slot[kP] = 3; }
@@ -432,8 +509,11 @@ int solar_gpu_init(const solar_desc* d, solar_ctx** out) {
   TRY(upload_constants());
   if (c->fp32) TRY(upload_tables<float>(c));
   else TRY(upload_tables<double>(c));
-  TRYC(cudaMalloc((void**)&c->dt.s0, c->ht.s0.size() * sizeof(int)));
-  TRYC(cudaMemcpy(c->dt.s0, c->ht.s0.data(), c->ht.s0.size() * sizeof(int), cudaMemcpyHostToDevice));
+  TRYC(cudaMalloc((void**)&c->dt.esrc, c->ht.esrc.size() * sizeof(int)));
+  TRYC(cudaMemcpy(c->dt.esrc, c->ht.esrc.data(), c->ht.esrc.size() * sizeof(int), cudaMemcpyHostToDevice));
+  TRYC(cudaMalloc((void**)&c->err, sizeof(int)));
+  TRYC(cudaMemset(c->err, 0, sizeof(int)));
+  if (!tensor_map_encoder()) { solar_gpu_finalize(c); return fail(SOLAR_ERR_CUDA, "cuTensorMapEncodeTiled entry point unavailable"); }
   TRY(upload<double>((void**)&c->dt.rad64, c->ht.radial));
   {
     std::vector<double> vol2(c->ht.metric.begin() + (size_t)kMVol * g.n * g.n,
@@ -503,7 +583,7 @@ int solar_gpu_rk4(solar_ctx* c, int nsteps) {
   if ((rc = capture_step_graph(c))) return rc;
   for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(c->step_graph, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  return SOLAR_OK;
+  return check_device_error(c);
 }
 
 int solar_gpu_rk4_runs(solar_ctx* c, const int* nsteps_per_run) {
@@ -521,7 +601,7 @@ int solar_gpu_rk4_runs(solar_ctx* c, const int* nsteps_per_run) {
   if ((rc = capture_batch_graph(c))) return rc;
   for (int s = 0; s < maxs; ++s) CK(cudaGraphLaunch(c->batch_graph, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  return SOLAR_OK;
+  return check_device_error(c);
 }
 
 // Operator-level drop-ins: inputs go to buffer B (run 0), results come from buffer W.
@@ -536,9 +616,11 @@ int solar_gpu_compute_rhs(solar_ctx* c, const double* q, double* rhs) {
   if (rc) return rc;
   if (!q || !rhs) return fail(SOLAR_ERR_ARG, "null array");
   if ((rc = op_prepare_state(c, q))) return rc;
-  if (c->fp32) { launch_edge<float>(c, c->B, 0, nullptr); launch_stage<float>(c, c->B, c->W, 2, 0, nullptr); }
-  else { launch_edge<double>(c, c->B, 0, nullptr); launch_stage<double>(c, c->B, c->W, 2, 0, nullptr); }
+  if (c->fp32) { launch_edge<float>(c, c->B, 0, nullptr); rc = launch_stage<float>(c, c->B, c->W, 2, 0, nullptr); }
+  else { launch_edge<double>(c, c->B, 0, nullptr); rc = launch_stage<double>(c, c->B, c->W, 2, 0, nullptr); }
+  if (rc) return rc;
   CK(cudaGetLastError());
+  if ((rc = check_device_error(c))) return rc;
   return download_fields(c, c->W, 0, rhs, 5, kAllFields, 5);
 }
 
@@ -564,9 +646,11 @@ int solar_gpu_filter_exp(solar_ctx* c, const double* q, double* qf) {
   if (rc) return rc;
   if (!q || !qf) return fail(SOLAR_ERR_ARG, "null array");
   if ((rc = op_prepare_state(c, q))) return rc;
-  if (c->fp32) { launch_edge<float>(c, c->B, 1, nullptr); launch_filter<float>(c, c->B, c->W, nullptr); }
-  else { launch_edge<double>(c, c->B, 1, nullptr); launch_filter<double>(c, c->B, c->W, nullptr); }
+  if (c->fp32) { launch_edge<float>(c, c->B, 1, nullptr); rc = launch_filter<float>(c, c->B, c->W, nullptr); }
+  else { launch_edge<double>(c, c->B, 1, nullptr); rc = launch_filter<double>(c, c->B, c->W, nullptr); }
+  if (rc) return rc;
   CK(cudaGetLastError());
+  if ((rc = check_device_error(c))) return rc;
   return download_fields(c, c->W, 0, qf, 5, kAllFields, 5);
 }
 
@@ -583,9 +667,11 @@ static int grad_div_op(solar_ctx* c, const double* fields[4], double* outs[4]) {
       for (int z = 0; z < 6; ++z)
         std::memcpy(&q[((size_t)z * 5 + ref[m]) * V], fields[m] + (size_t)z * V, V * sizeof(double));
   if ((rc = op_prepare_state(c, q.data()))) return rc;
-  if (c->fp32) { launch_edge<float>(c, c->B, 0, nullptr); launch_stage<float>(c, c->B, c->W, 3, 0, nullptr); }
-  else { launch_edge<double>(c, c->B, 0, nullptr); launch_stage<double>(c, c->B, c->W, 3, 0, nullptr); }
+  if (c->fp32) { launch_edge<float>(c, c->B, 0, nullptr); rc = launch_stage<float>(c, c->B, c->W, 3, 0, nullptr); }
+  else { launch_edge<double>(c, c->B, 0, nullptr); rc = launch_stage<double>(c, c->B, c->W, 3, 0, nullptr); }
+  if (rc) return rc;
   CK(cudaGetLastError());
+  if ((rc = check_device_error(c))) return rc;
   for (int m = 0; m < 4; ++m) {
     if (!outs[m]) continue;
     const int f = ref[m];
@@ -646,11 +732,12 @@ int solar_gpu_time_rk4(solar_ctx* c, int nsteps, int per_kernel, double* out7) {
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
     out7[0] = ms;
-    return SOLAR_OK;
+    return check_device_error(c);
   }
   std::vector<cudaEvent_t> evs;
   CK(cudaEventRecord(c->ev[0], c->stream));
-  for (int s = 0; s < nsteps; ++s) enqueue_step_any(c, nullptr, &evs);
+  for (int s = 0; s < nsteps; ++s)
+    if ((rc = enqueue_step_any(c, nullptr, &evs))) return rc;
   CK(cudaEventRecord(c->ev[1], c->stream));
   CK(cudaEventSynchronize(c->ev[1]));
   float ms = 0;
@@ -681,7 +768,7 @@ int solar_gpu_time_rk4(solar_ctx* c, int nsteps, int per_kernel, double* out7) {
   if (out7[4] > 0) out7[1] /= out7[4];
   if (out7[5] > 0) out7[2] /= out7[5];
   if (out7[6] > 0) out7[3] /= out7[6];
-  return SOLAR_OK;
+  return check_device_error(c);
 }
 
 int solar_gpu_synchronize(solar_ctx* c) {
