@@ -72,11 +72,10 @@ template <> struct Coef<float> {
 
 // ---------------------------------------------------------------------------------
 // Edge (ghost) kernel: INTERPOLATE_ALONG_X/Y + TRANSFORM_VECTOR_BETWEEN_MESHES_DIV + the
-// inter-zone exchange and its reversal, in one pass.  Each thread owns one ghost point
-// (receiver face, edge, layer, position along the edge) and walks a chunk of radial planes.
-// Its 9 source points and coefficients are loaded once: the scalar weights are the
-// Lagrange weights; the vector coefficients fold the Lagrange weight, the source face's
-// (xi,eta)->(theta,phi) conversion and the receiver-frame rotation into one pair per tap.
+// inter-zone exchange and its reversal, in one pass.  Every ghost value is a 9-tap sum
+// over one source line: the scalar weights are the Lagrange weights; the vector
+// coefficients fold the Lagrange weight, the source face's (xi,eta)->(theta,phi)
+// conversion and the receiver-frame rotation into one pair per tap.
 // mode 0: RHS halos -- p scalar on all edges; v_xi on W/E and v_eta on S/N, rotated.
 // mode 1: filter halos -- every stored field, scalar, all edges (filter.f90:23-28).
 template <typename T>
@@ -91,70 +90,92 @@ struct EdgeArgs {
   int kchunk;
 };
 
+// One CTA per (run, receiving face and edge, chunk of kc planes).  The source face's three
+// edge lines (rows 1..3 / n-4..n-2, or the same columns) of every needed field are first
+// staged in shared memory with coalesced loads -- columns are read three values per row --
+// then every ghost value is a 9-tap sum over shared memory with its folded coefficients.
 template <typename T>
-__global__ void __launch_bounds__(192) edge_kernel(const EdgeArgs<T> a) {
+__global__ void __launch_bounds__(256) edge_kernel(const EdgeArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char esm[];
+  T* buf = reinterpret_cast<T*>(esm);                    // [field][kk][layer][t_s]
   const Geom& g = a.g;
   const int n = g.n;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;   // position along the edge
-  const int l = threadIdx.y;                             // ghost layer 0..2
-  const int z = blockIdx.z;                              // (run*6 + face)*4 + edge
-  const int e = z & 3, face = (z >> 2) % 6, run = (z >> 2) / 6;
-  if (t >= n) return;
+  const int fe = blockIdx.y, face = fe >> 2, e = fe & 3, run = blockIdx.z;
   if (a.active && !a.active[run]) return;
-  const int kb = blockIdx.y * a.kchunk;
-  const int ke = min(g.nr, kb + a.kchunk);
+  const int kb = blockIdx.x * a.kchunk;
+  if (kb >= g.nr) return;
+  const int kc = min(a.kchunk, g.nr - kb);
   const EdgeRouteDev rt = cRoute[face][e];
-  const long long row = ((((long long)face * 4 + e) * 3 + l) * n + t) * 9;
-  int off[9];
-  T w[9];
-#pragma unroll
-  for (int s = 0; s < 9; ++s) {
-    const int p2 = a.esrc[row + s];
-    off[s] = (JOFF + p2 / n) * g.pitch + IOFF + p2 % n;
-    w[s] = a.ew[row + s];
-  }
-  int dst;
-  if (e == 0) dst = (JOFF - 1 - l) * g.pitch + IOFF + t;
-  else if (e == 1) dst = (JOFF + n + l) * g.pitch + IOFF + t;
-  else if (e == 2) dst = (JOFF + t) * g.pitch + IOFF - 1 - l;
-  else dst = (JOFF + t) * g.pitch + IOFF + n + l;
-  if (a.mode == 1) {
-    for (int s = 0; s < g.nf; ++s) {
-      const T* src = a.q + g.vol(run, rt.src_face, s);
-      T* out = a.q + g.vol(run, face, s);
-      for (int k = kb; k < ke; ++k) {
-        const long long kp = (long long)k * g.plane;
-        T acc = T(0);
-#pragma unroll
-        for (int m = 0; m < 9; ++m) acc = fma(w[m], __ldg(src + kp + off[m]), acc);
-        out[kp + dst] = acc;
+  const bool along_i = rt.src_edge <= 1;                 // S/N source lines run along i
+  const bool low = (rt.src_edge == 0 || rt.src_edge == 2);
+  const int nfl = a.mode == 1 ? g.nf : 3;                // staged fields
+  auto slot_of = [&](int f) {
+    return a.mode == 1 ? f : (f == 0 ? g.slot[kP] : (f == 1 ? g.slot[kVxi] : g.slot[kVeta]));
+  };
+  for (int fk = 0; fk < nfl * kc; ++fk) {               // uniform over the CTA
+    const int f = fk / kc, kk = fk - f * kc;
+    const T* src = a.q + g.vol(run, rt.src_face, slot_of(f)) + (long long)(kb + kk) * g.plane;
+    T* dst = buf + (long long)fk * 3 * n;
+    if (along_i) {                                       // rows: coalesced along i
+      for (int l = 0; l < 3; ++l) {
+        const T* rowp = src + (long long)(JOFF + (low ? l + 1 : n - 2 - l)) * g.pitch + IOFF;
+        for (int t = threadIdx.x; t < n; t += blockDim.x) cp_async_small<sizeof(T)>(dst + l * n + t, rowp + t);
+      }
+    } else {                                             // columns: the three layers of a row together
+      for (int idx = threadIdx.x; idx < 3 * n; idx += blockDim.x) {
+        const int t = idx / 3, l = idx - 3 * t;
+        const int col = low ? l + 1 : n - 2 - l;
+        cp_async_small<sizeof(T)>(dst + l * n + t, src + (long long)(JOFF + t) * g.pitch + IOFF + col);
       }
     }
-    return;
   }
-  T gx[9], gy[9];
+  cp_async_wait_all();
+  __syncthreads();
+  for (int pr = threadIdx.x; pr < 3 * n; pr += blockDim.x) {
+    const int t = pr % n, l = pr / n;                    // receiver position and layer
+    const long long row = ((((long long)face * 4 + e) * 3 + l) * n + t) * 9;
+    const int p2 = a.esrc[row];
+    const int s0 = along_i ? p2 % n : p2 / n;             // first tap along the source edge
+    long long dst;
+    if (e == 0) dst = g.at(0, -1 - l, t);
+    else if (e == 1) dst = g.at(0, n + l, t);
+    else if (e == 2) dst = g.at(0, t, -1 - l);
+    else dst = g.at(0, t, n + l);
+    T w[9];
 #pragma unroll
-  for (int s = 0; s < 9; ++s) {
-    gx[s] = a.eg[(row + s) * 2 + 0];
-    gy[s] = a.eg[(row + s) * 2 + 1];
-  }
-  const T* sp = a.q + g.vol(run, rt.src_face, g.slot[kP]);
-  const T* sx = a.q + g.vol(run, rt.src_face, g.slot[kVxi]);
-  const T* sy = a.q + g.vol(run, rt.src_face, g.slot[kVeta]);
-  T* op = a.q + g.vol(run, face, g.slot[kP]);
-  T* ov = a.q + g.vol(run, face, (e >= 2) ? g.slot[kVxi] : g.slot[kVeta]);
-#pragma unroll 2
-  for (int k = kb; k < ke; ++k) {
-    const long long kp = (long long)k * g.plane;
-    T ap = T(0), av = T(0);
+    for (int s = 0; s < 9; ++s) w[s] = a.ew[row + s];
+    if (a.mode == 1) {
+      for (int f = 0; f < nfl; ++f) {
+        T* out = a.q + g.vol(run, face, slot_of(f));
+        for (int kk = 0; kk < kc; ++kk) {
+          const T* b = buf + ((f * kc + kk) * 3 + l) * n + s0;
+          T acc = T(0);
 #pragma unroll
-    for (int m = 0; m < 9; ++m) {
-      ap = fma(w[m], __ldg(sp + kp + off[m]), ap);
-      av = fma(gx[m], __ldg(sx + kp + off[m]), av);
-      av = fma(gy[m], __ldg(sy + kp + off[m]), av);
+          for (int s = 0; s < 9; ++s) acc = fma(w[s], b[s], acc);
+          out[(long long)(kb + kk) * g.plane + dst] = acc;
+        }
+      }
+      continue;
     }
-    op[kp + dst] = ap;
-    ov[kp + dst] = av;
+    T gx[9], gy[9];
+#pragma unroll
+    for (int s = 0; s < 9; ++s) { gx[s] = a.eg[(row + s) * 2]; gy[s] = a.eg[(row + s) * 2 + 1]; }
+    T* op = a.q + g.vol(run, face, g.slot[kP]);
+    T* ov = a.q + g.vol(run, face, (e >= 2) ? g.slot[kVxi] : g.slot[kVeta]);
+    for (int kk = 0; kk < kc; ++kk) {
+      const T* bp = buf + ((0 * kc + kk) * 3 + l) * n + s0;
+      const T* bx = buf + ((1 * kc + kk) * 3 + l) * n + s0;
+      const T* by = buf + ((2 * kc + kk) * 3 + l) * n + s0;
+      T ap = T(0), av = T(0);
+#pragma unroll
+      for (int s = 0; s < 9; ++s) {
+        ap = fma(w[s], bp[s], ap);
+        av = fma(gx[s], bx[s], av);
+        av = fma(gy[s], by[s], av);
+      }
+      op[(long long)(kb + kk) * g.plane + dst] = ap;
+      ov[(long long)(kb + kk) * g.plane + dst] = av;
+    }
   }
 }
 
@@ -181,7 +202,7 @@ enum { mD = 0, mXYD, mC, mXYC, mDivX, mDivY, mTX, mTY, mVol, mCount };
 // MODE 0: RK update, stages 2-5 (reads qw).  MODE 1: RK update, stage 1 (qw = 0).
 // MODE 2: write the raw COMPUTE_RHS into qout.  MODE 3: write (grad_xi, grad_eta,
 // grad_r, div) into the v_xi, v_eta, v_r, p slots of qout.
-constexpr int kLead = 8;
+constexpr int kLead = 7;
 constexpr int kTile = 3;
 
 template <typename T>
@@ -205,24 +226,56 @@ struct StageArgs {
 
 __host__ __device__ constexpr size_t align128(size_t b) { return (b + 127) / 128 * 128; }
 
-template <typename T, int TX, int TY>
+// 16-byte vectors: V = 4 floats or 2 doubles.
+template <typename T> struct Vec16;
+template <> struct Vec16<float> { using type = float4; static constexpr int V = 4; };
+template <> struct Vec16<double> { using type = double2; static constexpr int V = 2; };
+
+template <typename T>
+__device__ __forceinline__ void ldv(const T* p, T* out) {
+  using VT = typename Vec16<T>::type;
+  const VT v = *reinterpret_cast<const VT*>(p);
+  const T* e = reinterpret_cast<const T*>(&v);
+#pragma unroll
+  for (int q = 0; q < Vec16<T>::V; ++q) out[q] = e[q];
+}
+template <typename T>
+__device__ __forceinline__ void stv(T* p, const T* in) {
+  using VT = typename Vec16<T>::type;
+  VT v;
+  T* e = reinterpret_cast<T*>(&v);
+#pragma unroll
+  for (int q = 0; q < Vec16<T>::V; ++q) e[q] = in[q];
+  *reinterpret_cast<VT*>(p) = v;
+}
+
+template <typename T, int TX, int TY, bool HAS_RHO>
 struct StageLayout {
   static constexpr int PB = (TX + 8) * (TY + 6), XB = (TX + 8) * TY, YB = TX * (TY + 6), OB = TX * TY;
+  static constexpr int NO = HAS_RHO ? 6 : 4;                          // rho + qw boxes
   static constexpr size_t P_BYTES = align128(PB * sizeof(T));
   static constexpr size_t X_BYTES = align128(XB * sizeof(T));
   static constexpr size_t Y_BYTES = align128(YB * sizeof(T));
   static constexpr size_t O_BYTES = align128(OB * sizeof(T));
   static constexpr size_t LEAD = P_BYTES + O_BYTES;                    // p box + v_r
-  static constexpr size_t TILE = X_BYTES + Y_BYTES + 6 * O_BYTES;     // v_xi, v_eta, rho, 5 qw
+  static constexpr size_t TILE = X_BYTES + Y_BYTES + NO * O_BYTES;     // v_xi, v_eta, (rho), qw
   static constexpr size_t BAR = kLead * LEAD + kTile * TILE;
   static constexpr size_t TOTAL = BAR + (kLead + kTile) * sizeof(uint64_t);
 };
 
-template <typename T, int TX, int TY, int MODE>
-__global__ void __launch_bounds__(TX * TY, sizeof(T) == 8 ? 2 : 3) stage_kernel(const __grid_constant__ StageArgs<T> a) {
-  using L = StageLayout<T, TX, TY>;
+// Each thread owns V consecutive points of one row (V = 16 bytes / sizeof(T)), so the
+// CTA has (TX/V) x TY threads and every shared-memory access is a 16-byte vector.
+template <typename T, int TX, int TY, int MODE, bool HAS_RHO>
+__global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __grid_constant__ StageArgs<T> a) {
+  constexpr int V = Vec16<T>::V;
+  constexpr int NT = TX / V;
+  constexpr int NV = (V + 8) / V;            // vectors covering box columns c .. c+V+7
+  constexpr int PW = TX + 8;
+  constexpr int QOFF = HAS_RHO ? 1 : 0;      // first qw box inside a tile slot
+  using L = StageLayout<T, TX, TY, HAS_RHO>;
   extern __shared__ __align__(128) unsigned char smem[];
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L::BAR);
+  uint64_t* barL = reinterpret_cast<uint64_t*>(smem + L::BAR);
+  uint64_t* barT = barL + kLead;
   const Geom& g = a.g;
   const int n = g.n, nr = g.nr;
   const int tiles_x = n / TX;
@@ -232,173 +285,231 @@ __global__ void __launch_bounds__(TX * TY, sizeof(T) == 8 ? 2 : 3) stage_kernel(
   const int kb = blockIdx.y * a.kchunk;
   if (kb >= nr) return;
   const int ke = min(nr, kb + a.kchunk);
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-  const int i = i0 + tx, j = j0 + ty;
+  const int cx = threadIdx.x, ty = threadIdx.y, tid = ty * NT + cx;
   const int sP = g.slot[kP], sX = g.slot[kVxi], sY = g.slot[kVeta], sR = g.slot[kVr], sRho = g.slot[kRho];
-  const bool has_rho = sRho >= 0 && MODE != 3;
   const int zbase = (run * 6 + face) * g.nf;   // plane index of (slot s, k) = (zbase + s) * nr + k
   auto clampk = [nr](int k) { return min(max(k - 3, 0), nr - 7); };
   const int m_lo = clampk(kb), m_hi = clampk(ke - 1) + 6;
 
-  auto leadP = [&](int m) { return reinterpret_cast<T*>(smem + ((m - m_lo) % kLead) * L::LEAD); };
-  auto leadR = [&](int m) { return reinterpret_cast<T*>(smem + ((m - m_lo) % kLead) * L::LEAD + L::P_BYTES); };
-  auto tileBase = [&](int k) { return smem + kLead * L::LEAD + ((k - kb) % kTile) * L::TILE; };
-  auto tileX = [&](int k) { return reinterpret_cast<T*>(tileBase(k)); };
-  auto tileY = [&](int k) { return reinterpret_cast<T*>(tileBase(k) + L::X_BYTES); };
-  auto tileO = [&](int k, int q) { return reinterpret_cast<T*>(tileBase(k) + L::X_BYTES + L::Y_BYTES + q * L::O_BYTES); };
-  uint64_t* barL = bars;
-  uint64_t* barT = bars + kLead;
-
+  auto lead = [&](int slot) { return smem + slot * L::LEAD; };
+  auto tile = [&](int slot) { return smem + kLead * L::LEAD + slot * L::TILE; };
   const int xP = IOFF + i0 - 4, yP = JOFF + j0 - 3;   // p / v_xi boxes start 4 columns left
   const int xO = IOFF + i0, yO = JOFF + j0;
-  auto issue_lead = [&](int m) {
-    uint64_t* b = &barL[(m - m_lo) % kLead];
+  auto issue_lead = [&](int m, int slot) {
+    uint64_t* b = &barL[slot];
     mbar_expect_tx(b, (L::PB + L::OB) * sizeof(T));
-    tma_load_3d(leadP(m), &a.mP, xP, yP, (zbase + sP) * nr + m, b);
-    tma_load_3d(leadR(m), &a.mO, xO, yO, (zbase + sR) * nr + m, b);
+    tma_load_3d(lead(slot), &a.mP, xP, yP, (zbase + sP) * nr + m, b);
+    tma_load_3d(lead(slot) + L::P_BYTES, &a.mO, xO, yO, (zbase + sR) * nr + m, b);
   };
-  auto issue_tile = [&](int k) {
-    uint64_t* b = &barT[(k - kb) % kTile];
+  auto issue_tile = [&](int k, int slot) {
+    uint64_t* b = &barT[slot];
     uint32_t bytes = (L::XB + L::YB) * sizeof(T);
-    if (has_rho) bytes += L::OB * sizeof(T);
+    if (HAS_RHO && MODE != 3) bytes += L::OB * sizeof(T);
     if (MODE == 0) bytes += g.nf * L::OB * sizeof(T);
     mbar_expect_tx(b, bytes);
-    tma_load_3d(tileX(k), &a.mX, xP, yO, (zbase + sX) * nr + k, b);
-    tma_load_3d(tileY(k), &a.mY, xO, yP, (zbase + sY) * nr + k, b);
-    if (has_rho) tma_load_3d(tileO(k, 0), &a.mO, xO, yO, (zbase + sRho) * nr + k, b);
+    unsigned char* t = tile(slot);
+    tma_load_3d(t, &a.mX, xP, yO, (zbase + sX) * nr + k, b);
+    tma_load_3d(t + L::X_BYTES, &a.mY, xO, yP, (zbase + sY) * nr + k, b);
+    if (HAS_RHO && MODE != 3)
+      tma_load_3d(t + L::X_BYTES + L::Y_BYTES, &a.mO, xO, yO, (zbase + sRho) * nr + k, b);
     if (MODE == 0)
-      for (int s = 0; s < g.nf; ++s) tma_load_3d(tileO(k, 1 + s), &a.mW, xO, yO, (zbase + s) * nr + k, b);
+      for (int s = 0; s < g.nf; ++s)
+        tma_load_3d(t + L::X_BYTES + L::Y_BYTES + (QOFF + s) * L::O_BYTES, &a.mW, xO, yO, (zbase + s) * nr + k, b);
   };
 
   if (tid == 0) {
-    for (int q = 0; q < kLead + kTile; ++q) mbar_init(&bars[q], 1);
+    for (int q = 0; q < kLead + kTile; ++q) mbar_init(&barL[q], 1);
     mbar_fence_init();
   }
   __syncthreads();
-  int m_issued = m_lo;
+  // producer state (thread 0 only)
+  int m_issued = m_lo, slot_issue = 0;
   if (tid == 0) {
     tma_prefetch_desc(&a.mP);
-    for (; m_issued <= min(m_lo + kLead - 1, m_hi); ++m_issued) issue_lead(m_issued);
-    for (int k = kb; k < min(kb + kTile, ke); ++k) issue_tile(k);
+    for (; m_issued <= min(m_lo + kLead - 1, m_hi); ++m_issued) {
+      issue_lead(m_issued, slot_issue);
+      if (++slot_issue == kLead) slot_issue = 0;
+    }
+    for (int k = kb; k < min(kb + kTile, ke); ++k) issue_tile(k, k - kb);
   }
 
+  // per-point constants
   const long long P2 = (long long)n * n;
-  const int p2 = j * n + i;
-  const T m_D = a.met[mD * P2 + p2], m_XYD = a.met[mXYD * P2 + p2];
-  const T m_C = a.met[mC * P2 + p2], m_XYC = a.met[mXYC * P2 + p2];
-  const T m_DivX = a.met[mDivX * P2 + p2], m_DivY = a.met[mDivY * P2 + p2];
-  const T m_TX = a.met[mTX * P2 + p2], m_TY = a.met[mTY * P2 + p2];
+  const int ib = i0 + V * cx, j = j0 + ty;
+  const int p2 = j * n + ib;
+  T m_D[V], m_XYD[V], m_C[V], m_XYC[V], m_DivX[V], m_DivY[V], m_TX[V], m_TY[V];
+  ldv(a.met + mD * P2 + p2, m_D);
+  ldv(a.met + mXYD * P2 + p2, m_XYD);
+  ldv(a.met + mC * P2 + p2, m_C);
+  ldv(a.met + mXYC * P2 + p2, m_XYC);
+  ldv(a.met + mDivX * P2 + p2, m_DivX);
+  ldv(a.met + mDivY * P2 + p2, m_DivY);
+  ldv(a.met + mTX * P2 + p2, m_TX);
+  ldv(a.met + mTY * P2 + p2, m_TY);
   const T c1 = Coef<T>::drp(1), c2 = Coef<T>::drp(2), c3 = Coef<T>::drp(3);
-  const long long own = g.at(0, j, i);
-  constexpr int PW = TX + 8;
-  const int pc = (ty + 3) * PW + tx + 4;              // own point inside the p box
-
-  T pw[7], vw[7];
+  const long long own = g.at(0, j, ib);
+  T* outS[5];
+  T* qwS[5];
 #pragma unroll
-  for (int s = 0; s < 7; ++s) { pw[s] = T(0); vw[s] = T(0); }
-  int mq = m_lo;
+  for (int f = 0; f < 5; ++f) {
+    const int sl = g.slot[f] < 0 ? 0 : g.slot[f];
+    outS[f] = a.qout + g.vol(run, face, sl) + own;
+    qwS[f] = a.qw + g.vol(run, face, sl) + own;
+  }
+  const int pc = (ty + 3) * PW + V * cx;       // box row of the own points; own point q at column V*cx+4+q
+  const int xc = ty * PW + V * cx;
+  const int yc = (ty + 3) * TX + V * cx;
+  const int oc = ty * TX + V * cx;
+
+  T pw[7][V], vw[7][V];
+#pragma unroll
+  for (int s = 0; s < 7; ++s)
+#pragma unroll
+    for (int q = 0; q < V; ++q) { pw[s][q] = T(0); vw[s][q] = T(0); }
+  int mq = m_lo, slot_q = 0, slot_k = (kb - m_lo) % kLead, slot_t = 0;
+  uint32_t phase_q = 0, phase_t = 0;
   bool ok = true;
   for (int k = kb; k < ke; ++k) {
     const int ks = clampk(k);
     for (; mq <= ks + 6; ++mq) {
-      ok &= mbar_wait(&barL[(mq - m_lo) % kLead], ((mq - m_lo) / kLead) & 1, a.err, 1);
+      ok &= mbar_wait(&barL[slot_q], phase_q, a.err, 1);
+      const T* bp = reinterpret_cast<const T*>(lead(slot_q));
 #pragma unroll
-      for (int s = 0; s < 6; ++s) { pw[s] = pw[s + 1]; vw[s] = vw[s + 1]; }
-      pw[6] = leadP(mq)[pc];
-      vw[6] = leadR(mq)[ty * TX + tx];
-    }
-    ok &= mbar_wait(&barT[(k - kb) % kTile], ((k - kb) / kTile) & 1, a.err, 2);
-    const T* sp = leadP(k);
-    const T* sx = tileX(k);
-    const T* sy = tileY(k);
-    const T dpx = a.inv_dxi * (c1 * (sp[pc + 1] - sp[pc - 1]) + c2 * (sp[pc + 2] - sp[pc - 2]) +
-                               c3 * (sp[pc + 3] - sp[pc - 3]));
-    const T dpy = a.inv_dxi * (c1 * (sp[pc + PW] - sp[pc - PW]) + c2 * (sp[pc + 2 * PW] - sp[pc - 2 * PW]) +
-                               c3 * (sp[pc + 3 * PW] - sp[pc - 3 * PW]));
-    const int xc = ty * PW + tx + 4;
-    const T dvx = a.inv_dxi * (c1 * (sx[xc + 1] - sx[xc - 1]) + c2 * (sx[xc + 2] - sx[xc - 2]) +
-                               c3 * (sx[xc + 3] - sx[xc - 3]));
-    const int yc = (ty + 3) * TX + tx;
-    const T dvy = a.inv_dxi * (c1 * (sy[yc + TX] - sy[yc - TX]) + c2 * (sy[yc + 2 * TX] - sy[yc - 2 * TX]) +
-                               c3 * (sy[yc + 3 * TX] - sy[yc - 3 * TX]));
-    const T facr = a.rad[rFacR * nr + k];
-    T dpr, dvr;
-    if (k >= 3 && k <= nr - 4) {
-      dpr = facr * (c1 * (pw[4] - pw[2]) + c2 * (pw[5] - pw[1]) + c3 * (pw[6] - pw[0]));
-      dvr = facr * (c1 * (vw[4] - vw[2]) + c2 * (vw[5] - vw[1]) + c3 * (vw[6] - vw[0]));
-    } else {
-      const bool lo = k < 3;
-      const int brow = lo ? k : nr - 1 - k;
-      T a_ = T(0), b_ = T(0);
+      for (int s = 0; s < 6; ++s)
 #pragma unroll
-      for (int s = 0; s < 7; ++s) {
-        const T b = Coef<T>::bdy(brow, lo ? s : 6 - s);
-        a_ = fma(b, pw[s], a_);
-        b_ = fma(b, vw[s], b_);
-      }
-      dpr = lo ? facr * a_ : -facr * a_;
-      dvr = lo ? facr * b_ : -facr * b_;
+        for (int q = 0; q < V; ++q) { pw[s][q] = pw[s + 1][q]; vw[s][q] = vw[s + 1][q]; }
+      ldv(bp + pc + 4, pw[6]);
+      ldv(reinterpret_cast<const T*>(lead(slot_q) + L::P_BYTES) + oc, vw[6]);
+      if (++slot_q == kLead) { slot_q = 0; phase_q ^= 1; }
     }
+    ok &= mbar_wait(&barT[slot_t], phase_t, a.err, 2);
+    const T* sp = reinterpret_cast<const T*>(lead(slot_k));
+    const unsigned char* tb = tile(slot_t);
+    const T* sx = reinterpret_cast<const T*>(tb);
+    const T* sy = reinterpret_cast<const T*>(tb + L::X_BYTES);
+    // xi windows of p and v_xi; eta columns of p and v_eta
+    T wp[NV * V], wx[NV * V];
+#pragma unroll
+    for (int m = 0; m < NV; ++m) { ldv(sp + pc + m * V, wp + m * V); ldv(sx + xc + m * V, wx + m * V); }
+    T pu[3][V], pd[3][V], yu[3][V], yd[3][V], vyo[V];
+#pragma unroll
+    for (int d = 1; d <= 3; ++d) {
+      ldv(sp + pc + 4 + d * PW, pu[d - 1]);
+      ldv(sp + pc + 4 - d * PW, pd[d - 1]);
+      ldv(sy + yc + d * TX, yu[d - 1]);
+      ldv(sy + yc - d * TX, yd[d - 1]);
+    }
+    ldv(sy + yc, vyo);
+    T rho[V], qwv[5][V];
+    if (HAS_RHO && MODE != 3) ldv(reinterpret_cast<const T*>(tb + L::X_BYTES + L::Y_BYTES) + oc, rho);
+    if (MODE == 0)
+#pragma unroll
+      for (int f = 0; f < 5; ++f)
+        if (f != kRho || HAS_RHO) {
+          const int sl = HAS_RHO ? f : f - 1;
+          ldv(reinterpret_cast<const T*>(tb + L::X_BYTES + L::Y_BYTES + (QOFF + sl) * L::O_BYTES) + oc, qwv[f]);
+        }
+    const T facr = __ldg(a.rad + rFacR * nr + k);
+    const T invr = __ldg(a.rad + rInvR * nr + k);
+    const bool interior = k >= 3 && k <= nr - 4;
     const int offk = k - ks;
-    T vr = vw[0];
+    const int brow = k < 3 ? k : nr - 1 - k;
+    T r_p[V], r_vx[V], r_ve[V], r_vr[V], r_rho[V], vr[V], pv[V], vxv[V];
+    T o0[V], o1[V], o2[V], o3[V];
 #pragma unroll
-    for (int s = 1; s < 7; ++s) vr = (offk == s) ? vw[s] : vr;
-    const T p = sp[pc];
-    const T vxi = sx[xc];
-    const T veta = sy[yc];
-    const T invr = a.rad[rInvR * nr + k];
-    const T gxi = invr * (m_D * dpx + m_XYD * dpy);
-    const T geta = invr * (m_C * dpy + m_XYC * dpx);
-    const T div = invr * (m_DivX * dvx + m_DivY * dvy - m_TX * vxi - m_TY * veta) + dvr + T(2) * vr * invr;
-    const long long pt = (long long)k * g.plane + own;
-    if (MODE == 3) {
-      a.qout[g.vol(run, face, sX) + pt] = gxi;
-      a.qout[g.vol(run, face, sY) + pt] = geta;
-      a.qout[g.vol(run, face, sR) + pt] = dpr;
-      a.qout[g.vol(run, face, sP) + pt] = div;
-    } else {
-      const T rho0 = a.rad[rRho0 * nr + k], inv_rho0 = a.rad[rInvRho0 * nr + k];
-      T c2rho0 = a.rad[rC2Rho0 * nr + k];
-      if (a.c2) c2rho0 = a.c2[((long long)face * nr + k) * P2 + p2] * rho0;
-      const int oc = ty * TX + tx;
-      const T rho = has_rho ? tileO(k, 0)[oc] : T(0);
-      T r_rho = -rho0 * div - vr * a.rad[rDRho0 * nr + k];
-      T r_vx = -gxi * inv_rho0;
-      T r_ve = -geta * inv_rho0;
-      T r_vr = -dpr * inv_rho0 - rho * a.rad[rG0Rho0 * nr + k];
-      T r_p = -c2rho0 * div + a.rad[rRho0G0 * nr + k] * vr;
-      if (MODE == 2) {
-        if (has_rho) a.qout[g.vol(run, face, sRho) + pt] = r_rho;
-        a.qout[g.vol(run, face, sX) + pt] = r_vx;
-        a.qout[g.vol(run, face, sY) + pt] = r_ve;
-        a.qout[g.vol(run, face, sR) + pt] = r_vr;
-        a.qout[g.vol(run, face, sP) + pt] = r_p;
+    for (int q = 0; q < V; ++q) {
+      const T dpx = a.inv_dxi * (c1 * (wp[5 + q] - wp[3 + q]) + c2 * (wp[6 + q] - wp[2 + q]) + c3 * (wp[7 + q] - wp[1 + q]));
+      const T dpy = a.inv_dxi * (c1 * (pu[0][q] - pd[0][q]) + c2 * (pu[1][q] - pd[1][q]) + c3 * (pu[2][q] - pd[2][q]));
+      const T dvx = a.inv_dxi * (c1 * (wx[5 + q] - wx[3 + q]) + c2 * (wx[6 + q] - wx[2 + q]) + c3 * (wx[7 + q] - wx[1 + q]));
+      const T dvy = a.inv_dxi * (c1 * (yu[0][q] - yd[0][q]) + c2 * (yu[1][q] - yd[1][q]) + c3 * (yu[2][q] - yd[2][q]));
+      T dpr, dvr, v_r;
+      if (interior) {
+        dpr = facr * (c1 * (pw[4][q] - pw[2][q]) + c2 * (pw[5][q] - pw[1][q]) + c3 * (pw[6][q] - pw[0][q]));
+        dvr = facr * (c1 * (vw[4][q] - vw[2][q]) + c2 * (vw[5][q] - vw[1][q]) + c3 * (vw[6][q] - vw[0][q]));
+        v_r = vw[3][q];
       } else {
-        // BC_RHS (bc_acoustic_wave.f90:432-452) then SPONGE (sponge.f90:502-504)
-        if (k == 0 || k == nr - 1) { r_rho = r_vx = r_ve = r_vr = r_p = T(0); }
-        const T sig = a.rad[rSigma * nr + k];
-        r_rho -= sig * rho;
-        r_vr -= sig * vr;
-        r_p -= sig * p;
-        // qw = alpha qw + dt rhs ; q = q + beta qw   (timestep.f90:68-69)
-        auto update = [&](int s, T q, T r) {
-          const T w = (MODE == 1) ? a.dt * r : fma(a.alpha, tileO(k, 1 + s)[oc], a.dt * r);
-          a.qw[g.vol(run, face, s) + pt] = w;
-          a.qout[g.vol(run, face, s) + pt] = fma(a.beta, w, q);
-        };
-        if (has_rho) update(sRho, rho, r_rho);
-        update(sX, vxi, r_vx);
-        update(sY, veta, r_ve);
-        update(sR, vr, r_vr);
-        update(sP, p, r_p);
+        const bool lo = k < 3;
+        T a_ = T(0), b_ = T(0);
+#pragma unroll
+        for (int s = 0; s < 7; ++s) {
+          const T b = Coef<T>::bdy(brow, lo ? s : 6 - s);
+          a_ = fma(b, pw[s][q], a_);
+          b_ = fma(b, vw[s][q], b_);
+        }
+        dpr = lo ? facr * a_ : -facr * a_;
+        dvr = lo ? facr * b_ : -facr * b_;
+        v_r = vw[0][q];
+#pragma unroll
+        for (int s = 1; s < 7; ++s) v_r = (offk == s) ? vw[s][q] : v_r;
       }
+      const T p = wp[4 + q], vxi = wx[4 + q], veta = vyo[q];
+      const T gxi = invr * (m_D[q] * dpx + m_XYD[q] * dpy);
+      const T geta = invr * (m_C[q] * dpy + m_XYC[q] * dpx);
+      const T div = invr * (m_DivX[q] * dvx + m_DivY[q] * dvy - m_TX[q] * vxi - m_TY[q] * veta) + dvr + T(2) * v_r * invr;
+      vr[q] = v_r; pv[q] = p; vxv[q] = vxi;
+      if (MODE == 3) {
+        o0[q] = gxi; o1[q] = geta; o2[q] = dpr; o3[q] = div;
+      } else {
+        const T rho0 = __ldg(a.rad + rRho0 * nr + k), inv_rho0 = __ldg(a.rad + rInvRho0 * nr + k);
+        T c2rho0 = __ldg(a.rad + rC2Rho0 * nr + k);
+        if (a.c2) c2rho0 = a.c2[((long long)face * nr + k) * P2 + p2 + q] * rho0;
+        r_vx[q] = -gxi * inv_rho0;
+        r_ve[q] = -geta * inv_rho0;
+        r_vr[q] = -dpr * inv_rho0;
+        r_p[q] = -c2rho0 * div + __ldg(a.rad + rRho0G0 * nr + k) * v_r;
+        if (HAS_RHO) {
+          r_rho[q] = -rho0 * div - v_r * __ldg(a.rad + rDRho0 * nr + k);
+          r_vr[q] -= rho[q] * __ldg(a.rad + rG0Rho0 * nr + k);
+        }
+      }
+    }
+    const long long kp = (long long)k * g.plane;
+    if (MODE == 3) {
+      stv(outS[kVxi] + kp, o0);
+      stv(outS[kVeta] + kp, o1);
+      stv(outS[kVr] + kp, o2);
+      stv(outS[kP] + kp, o3);
+    } else if (MODE == 2) {
+      if (HAS_RHO) stv(outS[kRho] + kp, r_rho);
+      stv(outS[kVxi] + kp, r_vx);
+      stv(outS[kVeta] + kp, r_ve);
+      stv(outS[kVr] + kp, r_vr);
+      stv(outS[kP] + kp, r_p);
+    } else {
+      // BC_RHS (bc_acoustic_wave.f90:432-452) then SPONGE (sponge.f90:502-504)
+      const bool bc = (k == 0 || k == nr - 1);
+      const T sig = __ldg(a.rad + rSigma * nr + k);
+      const T dt = a.dt, alpha = a.alpha, beta = a.beta;
+      // qw = alpha qw + dt rhs ; q = q + beta qw   (timestep.f90:68-69)
+      auto update = [&](int f, const T* qv, const T* rv, bool damped) {
+        T w[V], o[V];
+#pragma unroll
+        for (int q = 0; q < V; ++q) {
+          T r = bc ? T(0) : rv[q];
+          if (damped) r -= sig * qv[q];
+          w[q] = (MODE == 1) ? dt * r : fma(alpha, qwv[f][q], dt * r);
+          o[q] = fma(beta, w[q], qv[q]);
+        }
+        stv(qwS[f] + kp, w);
+        stv(outS[f] + kp, o);
+      };
+      if (HAS_RHO) update(kRho, rho, r_rho, true);
+      update(kVxi, vxv, r_vx, false);
+      update(kVeta, vyo, r_ve, false);
+      update(kVr, vr, r_vr, true);
+      update(kP, pv, r_p, true);
     }
     // every thread is done with lead plane k and tile plane k: refill their slots
     if (__syncthreads_or(!ok)) break;
     if (tid == 0) {
-      if (k + kTile < ke) issue_tile(k + kTile);
-      for (; m_issued <= min(k + kLead, m_hi); ++m_issued) issue_lead(m_issued);
+      if (k + kTile < ke) issue_tile(k + kTile, slot_t);
+      for (; m_issued <= min(k + kLead, m_hi); ++m_issued) {
+        issue_lead(m_issued, slot_issue);
+        if (++slot_issue == kLead) slot_issue = 0;
+      }
     }
+    if (++slot_t == kTile) { slot_t = 0; phase_t ^= 1; }
+    if (++slot_k == kLead) slot_k = 0;
   }
   if (!ok && tid == 0) {
     // a wait gave up: give copies still in flight a bounded time to land before exit
@@ -433,8 +544,16 @@ struct FilterLayout {
   static constexpr size_t TOTAL = BAR + kFiltRing * sizeof(uint64_t);
 };
 
+// Each thread owns V consecutive points of one row (V = 16 bytes / sizeof(T)); the CTA
+// has (TX/V) x TY threads.  Per plane: the xi filter of every row of the box (rows
+// outside the face keep the unfiltered halo) goes to shared memory with 16-byte loads
+// and stores, then each thread eta-filters its V points and pushes them into an 11-deep
+// register queue; the k loop is unrolled by 11 so the queue indices are constants.
 template <typename T, int TX, int TY>
-__global__ void __launch_bounds__(TX * TY) filter_kernel(const __grid_constant__ FilterArgs<T> a) {
+__global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) filter_kernel(const __grid_constant__ FilterArgs<T> a) {
+  constexpr int V = Vec16<T>::V;
+  constexpr int NT = TX / V;                 // threads per row
+  constexpr int NV = (V + 8) / V;            // vectors covering columns c-4 .. c+V+3
   using L = FilterLayout<T, TX, TY>;
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L::BAR);
@@ -445,17 +564,14 @@ __global__ void __launch_bounds__(TX * TY) filter_kernel(const __grid_constant__
   const int s = blockIdx.y;                  // stored field
   const int rf = blockIdx.z, run = rf / 6, face = rf % 6;
   if (a.active && !a.active[run]) return;
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-  const int i = i0 + tx, j = j0 + ty;
+  const int cx = threadIdx.x, ty = threadIdx.y, tid = ty * NT + cx;
   constexpr int PW = TX + 8;
-  auto box = [&](int k) { return reinterpret_cast<const T*>(smem + (k % kFiltRing) * L::P_BYTES); };
-  auto st = [&](int k) { return reinterpret_cast<T*>(smem + kFiltRing * L::P_BYTES + (k & 1) * L::S_BYTES); };
   const int z0 = ((run * 6 + face) * g.nf + s) * nr;
   const int xP = IOFF + i0 - 4, yP = JOFF + j0 - 3;
-  auto issue = [&](int k) {
-    uint64_t* b = &bars[k % kFiltRing];
+  auto issue = [&](int k, int slot) {
+    uint64_t* b = &bars[slot];
     mbar_expect_tx(b, L::PB * sizeof(T));
-    tma_load_3d(smem + (k % kFiltRing) * L::P_BYTES, &a.mP, xP, yP, z0 + k, b);
+    tma_load_3d(smem + slot * L::P_BYTES, &a.mP, xP, yP, z0 + k, b);
   };
   if (tid == 0) {
     for (int q = 0; q < kFiltRing; ++q) mbar_init(&bars[q], 1);
@@ -463,40 +579,72 @@ __global__ void __launch_bounds__(TX * TY) filter_kernel(const __grid_constant__
   }
   __syncthreads();
   if (tid == 0)
-    for (int k = 0; k < min(kFiltRing, nr); ++k) issue(k);
-  T* out = a.qout + g.vol(run, face, s);
-  const long long own = g.at(0, j, i);
+    for (int k = 0; k < min(kFiltRing, nr); ++k) issue(k, k);
+  T* out = a.qout + g.vol(run, face, s) + g.at(0, j0 + ty, i0 + V * cx);
   const T f0 = Coef<T>::filt(0), f1 = Coef<T>::filt(1), f2 = Coef<T>::filt(2), f3 = Coef<T>::filt(3);
-  T tq[11];
+  T tq[11][V];
 #pragma unroll
-  for (int m = 0; m < 11; ++m) tq[m] = T(0);
+  for (int m = 0; m < 11; ++m)
+#pragma unroll
+    for (int q = 0; q < V; ++q) tq[m][q] = T(0);
+  T zero[V];
+#pragma unroll
+  for (int q = 0; q < V; ++q) zero[q] = T(0);
   bool ok = true;
-  for (int k = 0; k < nr; ++k) {
-    ok &= mbar_wait(&bars[k % kFiltRing], (k / kFiltRing) & 1, a.err, 3);
-    const T* bx = box(k);
-    T* t1 = st(k);
-    for (int r = ty; r < TY + 6; r += TY) {
-      const int jr = j0 - 3 + r;
-      const T* row = bx + r * PW + tx + 4;
-      T v;
-      if (jr < 0 || jr >= n) v = row[0];
-      else v = f0 * row[0] + f1 * (row[-1] + row[1]) + f2 * (row[-2] + row[2]) + f3 * (row[-3] + row[3]);
-      t1[r * TX + tx] = v;
-    }
-    if (__syncthreads_or(!ok)) break;
-    if (tid == 0 && k + kFiltRing < nr) issue(k + kFiltRing);
-    const T* c = t1 + (ty + 3) * TX + tx;
-    const T t2 = f0 * c[0] + f1 * (c[-TX] + c[TX]) + f2 * (c[-2 * TX] + c[2 * TX]) + f3 * (c[-3 * TX] + c[3 * TX]);
+  int slot = 0;
+  uint32_t phase = 0;
+  for (int kb = 0; kb < nr && ok; kb += 11) {
 #pragma unroll
-    for (int m = 0; m < 10; ++m) tq[m] = tq[m + 1];
-    tq[10] = t2;
-    if (k >= 10) {
-      T v = Coef<T>::filtr(0) * tq[5];
+    for (int u = 0; u < 11; ++u) {
+      const int k = kb + u;
+      if (k >= nr) break;
+      ok &= mbar_wait(&bars[slot], phase, a.err, 3);
+      const T* bx = reinterpret_cast<const T*>(smem + slot * L::P_BYTES);
+      T* t1 = reinterpret_cast<T*>(smem + kFiltRing * L::P_BYTES + (k & 1) * L::S_BYTES);
+      // xi filter of the box rows (columns V*cx .. V*cx+V-1 of the tile)
+      for (int r = ty; r < TY + 6; r += TY) {
+        const int jr = j0 - 3 + r;
+        T w[NV * V];
 #pragma unroll
-      for (int m = 1; m <= 5; ++m) v += Coef<T>::filtr(m) * (tq[5 - m] + tq[5 + m]);
-      out[(long long)(k - 5) * g.plane + own] = v;
+        for (int m = 0; m < NV; ++m) ldv(bx + r * PW + V * cx + m * V, w + m * V);
+        // w[q'] holds box column V*cx + q'; the own point q sits at box column V*cx + 4 + q
+        constexpr int o = 4;
+        T v[V];
+        if (jr < 0 || jr >= n) {
+#pragma unroll
+          for (int q = 0; q < V; ++q) v[q] = w[o + q];
+        } else {
+#pragma unroll
+          for (int q = 0; q < V; ++q)
+            v[q] = f0 * w[o + q] + f1 * (w[o + q - 1] + w[o + q + 1]) + f2 * (w[o + q - 2] + w[o + q + 2]) +
+                   f3 * (w[o + q - 3] + w[o + q + 3]);
+        }
+        stv(t1 + r * TX + V * cx, v);
+      }
+      if (__syncthreads_or(!ok)) { ok = false; break; }
+      if (tid == 0 && k + kFiltRing < nr) issue(k + kFiltRing, slot);
+      if (++slot == kFiltRing) { slot = 0; phase ^= 1; }
+      // eta filter of this thread's V points (rows ty .. ty+6 of the xi-filtered tile)
+      T c[7][V];
+#pragma unroll
+      for (int m = 0; m < 7; ++m) ldv(t1 + (ty + m) * TX + V * cx, c[m]);
+#pragma unroll
+      for (int q = 0; q < V; ++q)
+        tq[u][q] = f0 * c[3][q] + f1 * (c[2][q] + c[4][q]) + f2 * (c[1][q] + c[5][q]) + f3 * (c[0][q] + c[6][q]);
+      if (k >= 10) {
+        // planes k-10 .. k sit at queue rows (u+1 .. u+11) % 11; the centre is k-5
+        T v[V];
+#pragma unroll
+        for (int q = 0; q < V; ++q) {
+          T acc = Coef<T>::filtr(0) * tq[(u + 6) % 11][q];
+#pragma unroll
+          for (int m = 1; m <= 5; ++m) acc += Coef<T>::filtr(m) * (tq[(u + 6 - m) % 11][q] + tq[(u + 6 + m) % 11][q]);
+          v[q] = acc;
+        }
+        stv(out + (long long)(k - 5) * g.plane, v);
+      }
+      if (k < 5 || k >= nr - 5) stv(out + (long long)k * g.plane, zero);
     }
-    if (k < 5 || k >= nr - 5) out[(long long)k * g.plane + own] = T(0);
   }
   if (!ok && tid == 0)
     for (int q = 0; q < 1000; ++q) __nanosleep(1000);

@@ -166,39 +166,52 @@ static int launch_edge(solar_ctx* c, void* buf, int mode, const int* active) {
   a.active = active;
   a.g = c->g;
   a.mode = mode;
-  a.kchunk = c->edge_kchunk;
-  dim3 block(64, 3);
-  dim3 grid((c->g.n + 63) / 64, (c->g.nr + a.kchunk - 1) / a.kchunk, c->g.nruns * 24);
-  edge_kernel<T><<<grid, block, 0, c->stream>>>(a);
+  // planes per CTA: as many as fit 48 KB of staged source lines, at most 8
+  const int nfl = mode == 1 ? c->g.nf : 3;
+  const size_t per_plane = (size_t)nfl * 3 * c->g.n * sizeof(T);
+  a.kchunk = (int)std::max<size_t>(1, std::min<size_t>(8, 49152 / per_plane));
+  const size_t smem = per_plane * a.kchunk;
+  dim3 grid((c->g.nr + a.kchunk - 1) / a.kchunk, 24, c->g.nruns);
+  edge_kernel<T><<<grid, 256, smem, c->stream>>>(a);
   return SOLAR_OK;
 }
 
-template <typename T, int TX, int TY, int MODE>
+template <typename T, int TX, int TY, int MODE, bool HAS_RHO>
 static int launch_stage_t(solar_ctx* c, StageArgs<T>& a, const void* qin) {
-  using L = StageLayout<T, TX, TY>;
+  using L = StageLayout<T, TX, TY, HAS_RHO>;
   if (!make_map(c, qin, TX + 8, TY + 6, &a.mP) || !make_map(c, qin, TX + 8, TY, &a.mX) ||
       !make_map(c, qin, TX, TY + 6, &a.mY) || !make_map(c, qin, TX, TY, &a.mO) ||
       !make_map(c, c->W, TX, TY, &a.mW))
     return fail(SOLAR_ERR_CUDA, "cuTensorMapEncodeTiled failed");
   static bool attr_set = false;
   if (!attr_set) {
-    CK(cudaFuncSetAttribute(stage_kernel<T, TX, TY, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::TOTAL));
+    CK(cudaFuncSetAttribute(stage_kernel<T, TX, TY, MODE, HAS_RHO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)L::TOTAL));
     attr_set = true;
   }
   const int nchunks = (c->g.nr + a.kchunk - 1) / a.kchunk;
   dim3 grid((c->g.n / TX) * (c->g.n / TY), nchunks, c->g.nruns * 6);
-  stage_kernel<T, TX, TY, MODE><<<grid, dim3(TX, TY), L::TOTAL, c->stream>>>(a);
+  stage_kernel<T, TX, TY, MODE, HAS_RHO><<<grid, dim3(TX / Vec16<T>::V, TY), L::TOTAL, c->stream>>>(a);
   return SOLAR_OK;
 }
 
 template <typename T, int TX, int TY>
 static int launch_stage_mode(solar_ctx* c, StageArgs<T>& a, const void* qin, int mode) {
+  const bool rho = c->g.slot[kRho] >= 0;
   switch (mode) {
-    case 0: return launch_stage_t<T, TX, TY, 0>(c, a, qin);
-    case 1: return launch_stage_t<T, TX, TY, 1>(c, a, qin);
-    case 2: return launch_stage_t<T, TX, TY, 2>(c, a, qin);
-    default: return launch_stage_t<T, TX, TY, 3>(c, a, qin);
+    case 0: return rho ? launch_stage_t<T, TX, TY, 0, true>(c, a, qin) : launch_stage_t<T, TX, TY, 0, false>(c, a, qin);
+    case 1: return rho ? launch_stage_t<T, TX, TY, 1, true>(c, a, qin) : launch_stage_t<T, TX, TY, 1, false>(c, a, qin);
+    case 2: return rho ? launch_stage_t<T, TX, TY, 2, true>(c, a, qin) : launch_stage_t<T, TX, TY, 2, false>(c, a, qin);
+    default: return rho ? launch_stage_t<T, TX, TY, 3, true>(c, a, qin) : launch_stage_t<T, TX, TY, 3, false>(c, a, qin);
   }
+}
+
+// Stage tiles (TX x TY points).  The default is 32 x 16 in float and 32 x 8 in double;
+// 16 x 16 when nx is not a multiple of 32.
+static void default_tile(int n, bool fp32, int* tx, int* ty) {
+  if (n % 32) { *tx = 16; *ty = 16; return; }
+  *tx = 32;
+  *ty = fp32 ? 16 : 8;
 }
 
 template <typename T>
@@ -218,15 +231,13 @@ static int launch_stage(solar_ctx* c, const void* qin, void* qout, int mode, int
   a.beta = (T)kBeta[stage];
   a.inv_dxi = (T)(1.0 / c->ht.dxi);
   a.kchunk = c->kchunk;
-  if (mode >= 2) {  // operator-level calls use the default tile
-    if (c->g.n % 32 == 0) return launch_stage_mode<T, 32, 8>(c, a, qin, mode);
-    return launch_stage_mode<T, 16, 8>(c, a, qin, mode);
-  }
-  if (c->tile_x == 16 && c->tile_y == 8) return launch_stage_mode<T, 16, 8>(c, a, qin, mode);
-  if (c->tile_x == 32 && c->tile_y == 4) return launch_stage_mode<T, 32, 4>(c, a, qin, mode);
-  if (c->tile_x == 64 && c->tile_y == 4) return launch_stage_mode<T, 64, 4>(c, a, qin, mode);
-  if (c->tile_x == 16 && c->tile_y == 16) return launch_stage_mode<T, 16, 16>(c, a, qin, mode);
-  return launch_stage_mode<T, 32, 8>(c, a, qin, mode);
+  int tx = c->tile_x, ty = c->tile_y;
+  if (mode >= 2) default_tile(c->g.n, c->fp32, &tx, &ty);   // operator-level calls
+  if (tx == 16 && ty == 16) return launch_stage_mode<T, 16, 16>(c, a, qin, mode);
+  if (tx == 32 && ty == 8) return launch_stage_mode<T, 32, 8>(c, a, qin, mode);
+  if (tx == 32 && ty == 16) return launch_stage_mode<T, 32, 16>(c, a, qin, mode);
+  if (tx == 64 && ty == 8) return launch_stage_mode<T, 64, 8>(c, a, qin, mode);
+  return fail(SOLAR_ERR_ARG, "unsupported stage tile %d x %d", tx, ty);
 }
 
 template <typename T, int TX, int TY>
@@ -244,14 +255,14 @@ static int launch_filter_t(solar_ctx* c, const void* qin, void* qout, const int*
     attr_set = true;
   }
   dim3 grid((c->g.n / TX) * (c->g.n / TY), c->g.nf, c->g.nruns * 6);
-  filter_kernel<T, TX, TY><<<grid, dim3(TX, TY), L::TOTAL, c->stream>>>(a);
+  filter_kernel<T, TX, TY><<<grid, dim3(TX / Vec16<T>::V, TY), L::TOTAL, c->stream>>>(a);
   return SOLAR_OK;
 }
 
 template <typename T>
 static int launch_filter(solar_ctx* c, const void* qin, void* qout, const int* active) {
-  if (c->g.n % 32 == 0) return launch_filter_t<T, 32, 8>(c, qin, qout, active);
-  return launch_filter_t<T, 16, 8>(c, qin, qout, active);
+  if (c->g.n % 32 == 0) return launch_filter_t<T, 32, 16>(c, qin, qout, active);
+  return launch_filter_t<T, 16, 16>(c, qin, qout, active);
 }
 
 // One full time step (timestep.f90:61-82) on every run.  With ev != nullptr each kernel
@@ -479,10 +490,15 @@ int solar_gpu_init(const solar_desc* d, solar_ctx** out) {
   g.nruns = d->nruns;
   if (g.nf == 5) { for (int f = 0; f < 5; ++f) g.slot[f] = f; }
   else { g.slot[kRho] = -1; g.slot[kVxi] = 0; g.slot[kVeta] = 1; g.slot[kVr] = 2; g.slot[kP] = 3; }
-  // tile choice
-  c->tile_x = d->tile_x ? d->tile_x : (g.n % 32 == 0 ? 32 : 16);
-  c->tile_y = d->tile_y ? d->tile_y : 8;
-  if (g.n % c->tile_x || g.n % c->tile_y) { solar_gpu_finalize(c); return fail(SOLAR_ERR_ARG, "tile does not divide nx"); }
+  // tile choice (16x16, 32x8, 32x16, 64x8)
+  default_tile(g.n, c->fp32, &c->tile_x, &c->tile_y);
+  if (d->tile_x) c->tile_x = d->tile_x;
+  if (d->tile_y) c->tile_y = d->tile_y;
+  {
+    const int tx = c->tile_x, ty = c->tile_y;
+    const bool known = (tx == 16 && ty == 16) || (tx == 32 && (ty == 8 || ty == 16)) || (tx == 64 && ty == 8);
+    if (!known || g.n % tx || g.n % ty) { delete c; return fail(SOLAR_ERR_ARG, "unsupported stage tile %d x %d for nx %d", tx, ty, g.n); }
+  }
   if (d->kchunk > 0) c->kchunk = d->kchunk;
   else {
     const long long blocks = 6LL * g.nruns * (g.n / c->tile_x) * (g.n / c->tile_y);
