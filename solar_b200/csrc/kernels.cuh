@@ -41,6 +41,15 @@ struct Geom {
   __host__ __device__ long long at(int k, int j, int i) const {
     return (long long)k * plane + (long long)(JOFF + j) * pitch + IOFF + i;
   }
+  // Edge-line buffer ("strips"): for every face, edge, stored field and plane, the three
+  // source lines next to the edge that the neighbouring faces interpolate from --
+  //   S: rows j = 1..3, N: rows j = n-2..n-4, W: columns i = 1..3, E: columns i = n-2..n-4
+  // stored as strips[run][face][edge][slot][k][layer][t] with t along the edge.  It is the
+  // send buffer of the reference's halo exchange (temp(:,:,:,1:2) in derivative.f90).
+  __host__ __device__ long long strip(int run, int face, int edge, int s, int k, int l) const {
+    return (((((long long)(run * 6 + face) * 4 + edge) * nf + s) * nr + k) * 3 + l) * n;
+  }
+  __host__ __device__ long long strips_size() const { return (long long)nruns * 6 * 4 * nf * nr * 3 * n; }
 };
 
 struct EdgeRouteDev { int src_face, src_edge, reversed; };
@@ -81,30 +90,33 @@ template <> struct Coef<float> {
 template <typename T>
 struct EdgeArgs {
   T* q;                     // buffer whose frames are filled (its interior is the source)
-  const T* ew;              // [6][4][3][n][9]
-  const T* eg;              // [6][4][3][n][9][2]
-  const int* esrc;          // [6][4][3][n][9]  source point j*n + i
+  const T* ew;              // [6][4][3][9][n]     scalar tap weights, position fastest
+  const T* eg;              // [6][4][3][9][2][n]  vector tap weights (v_xi, v_eta)
+  const int* s0t;           // [6][4][3][n]        first tap along the source edge
   const int* active;        // per-run flag or nullptr
   Geom g;
   int mode;
   int kchunk;
 };
 
-// One CTA per (run, receiving face and edge, chunk of kc planes).  The source face's three
-// edge lines (rows 1..3 / n-4..n-2, or the same columns) of every needed field are first
-// staged in shared memory with coalesced loads -- columns are read three values per row --
-// then every ghost value is a 9-tap sum over shared memory with its folded coefficients.
-template <typename T>
-__global__ void __launch_bounds__(256) edge_kernel(const EdgeArgs<T> a) {
+// One CTA per (run, receiving face and edge, chunk of up to KC planes).  The source face's
+// three edge lines of every needed field are staged in shared memory with asynchronous
+// copies (rows as 16-byte pieces, columns three values per row), then each thread
+// produces the ghost values of its (position, layer) pairs for all staged planes at
+// once, so the planes' tap sums run in parallel.  Coefficient tables are stored
+// position-fastest ([face][edge][layer][tap][position]) so every table load of a warp is
+// one contiguous segment.
+template <typename T, int KC>
+__global__ void __launch_bounds__(128) edge_kernel(const EdgeArgs<T> a) {
   extern __shared__ __align__(16) unsigned char esm[];
   T* buf = reinterpret_cast<T*>(esm);                    // [field][kk][layer][t_s]
   const Geom& g = a.g;
   const int n = g.n;
   const int fe = blockIdx.y, face = fe >> 2, e = fe & 3, run = blockIdx.z;
   if (a.active && !a.active[run]) return;
-  const int kb = blockIdx.x * a.kchunk;
+  const int kb = blockIdx.x * KC;
   if (kb >= g.nr) return;
-  const int kc = min(a.kchunk, g.nr - kb);
+  const int kc = min(KC, g.nr - kb);
   const EdgeRouteDev rt = cRoute[face][e];
   const bool along_i = rt.src_edge <= 1;                 // S/N source lines run along i
   const bool low = (rt.src_edge == 0 || rt.src_edge == 2);
@@ -115,11 +127,13 @@ __global__ void __launch_bounds__(256) edge_kernel(const EdgeArgs<T> a) {
   for (int fk = 0; fk < nfl * kc; ++fk) {               // uniform over the CTA
     const int f = fk / kc, kk = fk - f * kc;
     const T* src = a.q + g.vol(run, rt.src_face, slot_of(f)) + (long long)(kb + kk) * g.plane;
-    T* dst = buf + (long long)fk * 3 * n;
-    if (along_i) {                                       // rows: coalesced along i
-      for (int l = 0; l < 3; ++l) {
+    T* dst = buf + (long long)(f * KC + kk) * 3 * n;
+    if (along_i) {                                       // rows: 16-byte pieces
+      constexpr int W16 = 16 / sizeof(T);
+      for (int idx = threadIdx.x * W16; idx < 3 * n; idx += blockDim.x * W16) {
+        const int l = idx / n, t = idx - l * n;
         const T* rowp = src + (long long)(JOFF + (low ? l + 1 : n - 2 - l)) * g.pitch + IOFF;
-        for (int t = threadIdx.x; t < n; t += blockDim.x) cp_async_small<sizeof(T)>(dst + l * n + t, rowp + t);
+        cp_async_16(dst + idx, rowp + t);
       }
     } else {                                             // columns: the three layers of a row together
       for (int idx = threadIdx.x; idx < 3 * n; idx += blockDim.x) {
@@ -131,11 +145,11 @@ __global__ void __launch_bounds__(256) edge_kernel(const EdgeArgs<T> a) {
   }
   cp_async_wait_all();
   __syncthreads();
+  const long long fstr = (long long)KC * 3 * n;         // field stride inside buf
   for (int pr = threadIdx.x; pr < 3 * n; pr += blockDim.x) {
-    const int t = pr % n, l = pr / n;                    // receiver position and layer
-    const long long row = ((((long long)face * 4 + e) * 3 + l) * n + t) * 9;
-    const int p2 = a.esrc[row];
-    const int s0 = along_i ? p2 % n : p2 / n;             // first tap along the source edge
+    const int l = pr / n, t = pr - l * n;               // receiver layer and position
+    const long long crow = ((long long)fe * 3 + l) * 9;  // tap rows of this (face, edge, layer)
+    const int s0 = a.s0t[((long long)fe * 3 + l) * n + t];
     long long dst;
     if (e == 0) dst = g.at(0, -1 - l, t);
     else if (e == 1) dst = g.at(0, n + l, t);
@@ -143,38 +157,51 @@ __global__ void __launch_bounds__(256) edge_kernel(const EdgeArgs<T> a) {
     else dst = g.at(0, t, n + l);
     T w[9];
 #pragma unroll
-    for (int s = 0; s < 9; ++s) w[s] = a.ew[row + s];
+    for (int s = 0; s < 9; ++s) w[s] = a.ew[(crow + s) * n + t];
+    const int b0 = l * n + s0;
     if (a.mode == 1) {
       for (int f = 0; f < nfl; ++f) {
-        T* out = a.q + g.vol(run, face, slot_of(f));
-        for (int kk = 0; kk < kc; ++kk) {
-          const T* b = buf + ((f * kc + kk) * 3 + l) * n + s0;
-          T acc = T(0);
+        T* out = a.q + g.vol(run, face, slot_of(f)) + (long long)kb * g.plane + dst;
+        const T* bf = buf + f * fstr + b0;
 #pragma unroll
-          for (int s = 0; s < 9; ++s) acc = fma(w[s], b[s], acc);
-          out[(long long)(kb + kk) * g.plane + dst] = acc;
+        for (int kk = 0; kk < KC; ++kk) {
+          if (kk < kc) {
+            const T* b = bf + kk * 3 * n;
+            T a0 = T(0), a1 = T(0);
+#pragma unroll
+            for (int s = 0; s < 9; s += 2) a0 = fma(w[s], b[s], a0);
+#pragma unroll
+            for (int s = 1; s < 9; s += 2) a1 = fma(w[s], b[s], a1);
+            out[(long long)kk * g.plane] = a0 + a1;
+          }
         }
       }
       continue;
     }
     T gx[9], gy[9];
 #pragma unroll
-    for (int s = 0; s < 9; ++s) { gx[s] = a.eg[(row + s) * 2]; gy[s] = a.eg[(row + s) * 2 + 1]; }
-    T* op = a.q + g.vol(run, face, g.slot[kP]);
-    T* ov = a.q + g.vol(run, face, (e >= 2) ? g.slot[kVxi] : g.slot[kVeta]);
-    for (int kk = 0; kk < kc; ++kk) {
-      const T* bp = buf + ((0 * kc + kk) * 3 + l) * n + s0;
-      const T* bx = buf + ((1 * kc + kk) * 3 + l) * n + s0;
-      const T* by = buf + ((2 * kc + kk) * 3 + l) * n + s0;
-      T ap = T(0), av = T(0);
+    for (int s = 0; s < 9; ++s) {
+      gx[s] = a.eg[((crow + s) * 2 + 0) * n + t];
+      gy[s] = a.eg[((crow + s) * 2 + 1) * n + t];
+    }
+    T* op = a.q + g.vol(run, face, g.slot[kP]) + (long long)kb * g.plane + dst;
+    T* ov = a.q + g.vol(run, face, (e >= 2) ? g.slot[kVxi] : g.slot[kVeta]) + (long long)kb * g.plane + dst;
 #pragma unroll
-      for (int s = 0; s < 9; ++s) {
-        ap = fma(w[s], bp[s], ap);
-        av = fma(gx[s], bx[s], av);
-        av = fma(gy[s], by[s], av);
+    for (int kk = 0; kk < KC; ++kk) {
+      if (kk < kc) {
+        const T* bp = buf + b0 + kk * 3 * n;
+        const T* bx = bp + fstr;
+        const T* by = bx + fstr;
+        T ap = T(0), ax = T(0), ay = T(0);
+#pragma unroll
+        for (int s = 0; s < 9; ++s) {
+          ap = fma(w[s], bp[s], ap);
+          ax = fma(gx[s], bx[s], ax);
+          ay = fma(gy[s], by[s], ay);
+        }
+        op[(long long)kk * g.plane] = ap;
+        ov[(long long)kk * g.plane] = ax + ay;
       }
-      op[(long long)(kb + kk) * g.plane + dst] = ap;
-      ov[(long long)(kb + kk) * g.plane + dst] = av;
     }
   }
 }
@@ -643,11 +670,36 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) filter_kernel(const _
         }
         stv(out + (long long)(k - 5) * g.plane, v);
       }
-      if (k < 5 || k >= nr - 5) stv(out + (long long)k * g.plane, zero);
     }
+  }
+  // the five end planes at each radial end are zero (filter.f90:726-775)
+  for (int m = 0; m < 10; ++m) {
+    const int k = m < 5 ? m : nr - 10 + m;
+    stv(out + (long long)k * g.plane, zero);
   }
   if (!ok && tid == 0)
     for (int q = 0; q < 1000; ++q) __nanosleep(1000);
+}
+
+// Fill the strip buffer of a whole buffer from its interior (after host uploads).
+template <typename T>
+__global__ void strip_extract_kernel(const T* __restrict__ q, T* __restrict__ strips, Geom g) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= g.strips_size()) return;
+  const int n = g.n;
+  const int t = idx % n;
+  long long r = idx / n;
+  const int l = r % 3; r /= 3;
+  const int k = r % g.nr; r /= g.nr;
+  const int s = r % g.nf; r /= g.nf;
+  const int e = r % 4; r /= 4;
+  const int face = r % 6, run = (int)(r / 6);
+  int ii, jj;
+  if (e == 0) { ii = t; jj = l + 1; }
+  else if (e == 1) { ii = t; jj = n - 2 - l; }
+  else if (e == 2) { ii = l + 1; jj = t; }
+  else { ii = n - 2 - l; jj = t; }
+  strips[idx] = q[g.vol(run, face, s) + g.at(k, jj, ii)];
 }
 
 // ---------------------------------------------------------------------------------

@@ -41,9 +41,9 @@ struct DevTables {
   void* rad = nullptr;     // T [kNumRadial][nr]
   void* met = nullptr;     // T [kNumMetric][n][n]
   void* conv = nullptr;    // T [3][4][n][n]
-  void* ew = nullptr;      // T [6][4][3][n][9]     folded edge weights (scalar)
-  void* eg = nullptr;      // T [6][4][3][n][9][2]  folded edge weights (vector)
-  int* esrc = nullptr;     // [6][4][3][n][9]
+  void* ew = nullptr;      // T [6][4][3][9][n]     folded edge weights (scalar)
+  void* eg = nullptr;      // T [6][4][3][9][2][n]  folded edge weights (vector)
+  int* s0t = nullptr;      // [6][4][3][n]          first tap of every ghost point
   void* c2 = nullptr;      // T [6][nr][n][n] optional
   double* rad64 = nullptr; // FP64 copies for diagnostics
   double* vol2 = nullptr;  // [n][n]
@@ -156,23 +156,29 @@ static bool make_map(const solar_ctx* c, const void* base, int bx, int by, CUten
   return r == CUDA_SUCCESS;
 }
 
+constexpr int kEdgePlanes = 4;   // radial planes per edge-kernel CTA
+
 template <typename T>
 static int launch_edge(solar_ctx* c, void* buf, int mode, const int* active) {
   EdgeArgs<T> a;
   a.q = (T*)buf;
   a.ew = (const T*)c->dt.ew;
   a.eg = (const T*)c->dt.eg;
-  a.esrc = c->dt.esrc;
+  a.s0t = c->dt.s0t;
   a.active = active;
   a.g = c->g;
   a.mode = mode;
-  // planes per CTA: as many as fit 48 KB of staged source lines, at most 8
   const int nfl = mode == 1 ? c->g.nf : 3;
-  const size_t per_plane = (size_t)nfl * 3 * c->g.n * sizeof(T);
-  a.kchunk = (int)std::max<size_t>(1, std::min<size_t>(8, 49152 / per_plane));
-  const size_t smem = per_plane * a.kchunk;
-  dim3 grid((c->g.nr + a.kchunk - 1) / a.kchunk, 24, c->g.nruns);
-  edge_kernel<T><<<grid, 256, smem, c->stream>>>(a);
+  const size_t smem = (size_t)nfl * kEdgePlanes * 3 * c->g.n * sizeof(T);
+  if (smem > 48 * 1024) {
+    static bool attr_set = false;
+    if (!attr_set) {
+      CK(cudaFuncSetAttribute(edge_kernel<T, kEdgePlanes>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+      attr_set = true;
+    }
+  }
+  dim3 grid((c->g.nr + kEdgePlanes - 1) / kEdgePlanes, 24, c->g.nruns);
+  edge_kernel<T, kEdgePlanes><<<grid, 128, smem, c->stream>>>(a);
   return SOLAR_OK;
 }
 
@@ -448,7 +454,7 @@ int solar_gpu_finalize(solar_ctx* c) {
   if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
   if (c->batch_graph) cudaGraphExecDestroy(c->batch_graph);
   void* ptrs[] = {c->A, c->B, c->W, c->stage64, c->part, c->red_out, c->active, c->target, c->done,
-                  c->err, c->dt.rad, c->dt.met, c->dt.ew, c->dt.eg, c->dt.esrc, c->dt.c2,
+                  c->err, c->dt.rad, c->dt.met, c->dt.ew, c->dt.eg, c->dt.s0t, c->dt.c2,
                   c->dt.rad64, c->dt.vol2, c->dt.drw, c->dt.c2_64, c->dt.tanx, c->dt.gr};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -516,6 +522,7 @@ int solar_gpu_init(const solar_desc* d, solar_ctx** out) {
   TRYC(cudaMemset(c->A, 0, bytes));
   TRYC(cudaMemset(c->B, 0, bytes));
   TRYC(cudaMemset(c->W, 0, bytes));
+
   TRYC(cudaMalloc((void**)&c->stage64, (size_t)vol_compact(c) * sizeof(double)));
   TRYC(cudaMalloc((void**)&c->part, (size_t)6 * g.nr * 5 * sizeof(double)));
   TRYC(cudaMalloc((void**)&c->red_out, 5 * sizeof(double)));
@@ -525,8 +532,8 @@ int solar_gpu_init(const solar_desc* d, solar_ctx** out) {
   TRY(upload_constants());
   if (c->fp32) TRY(upload_tables<float>(c));
   else TRY(upload_tables<double>(c));
-  TRYC(cudaMalloc((void**)&c->dt.esrc, c->ht.esrc.size() * sizeof(int)));
-  TRYC(cudaMemcpy(c->dt.esrc, c->ht.esrc.data(), c->ht.esrc.size() * sizeof(int), cudaMemcpyHostToDevice));
+  TRYC(cudaMalloc((void**)&c->dt.s0t, c->ht.s0t.size() * sizeof(int)));
+  TRYC(cudaMemcpy(c->dt.s0t, c->ht.s0t.data(), c->ht.s0t.size() * sizeof(int), cudaMemcpyHostToDevice));
   TRYC(cudaMalloc((void**)&c->err, sizeof(int)));
   TRYC(cudaMemset(c->err, 0, sizeof(int)));
   if (!tensor_map_encoder()) { solar_gpu_finalize(c); return fail(SOLAR_ERR_CUDA, "cuTensorMapEncodeTiled entry point unavailable"); }
@@ -623,8 +630,7 @@ int solar_gpu_rk4_runs(solar_ctx* c, const int* nsteps_per_run) {
 // Operator-level drop-ins: inputs go to buffer B (run 0), results come from buffer W.
 // The state buffer A is left untouched.
 static int op_prepare_state(solar_ctx* c, const double* q) {
-  int rc = upload_fields(c, c->B, 0, q, 5, kAllFields, 5);
-  return rc;
+  return upload_fields(c, c->B, 0, q, 5, kAllFields, 5);
 }
 
 int solar_gpu_compute_rhs(solar_ctx* c, const double* q, double* rhs) {

@@ -260,19 +260,21 @@ int build_tables(const solar_desc& d, HostTables& t, std::string& err) {
       }
     }
 
-  // Fold everything an edge value needs into one row of coefficients per ghost point.
-  t.ew.assign((size_t)6 * 4 * 3 * n * 9, 0.0);
-  t.eg.assign((size_t)6 * 4 * 3 * n * 9 * 2, 0.0);
-  t.esrc.assign((size_t)6 * 4 * 3 * n * 9, 0);
+  // Fold everything an edge value needs into one set of coefficients per ghost point.
+  t.ew.assign((size_t)6 * 4 * 3 * 9 * n, 0.0);
+  t.eg.assign((size_t)6 * 4 * 3 * 9 * 2 * n, 0.0);
+  t.s0t.assign((size_t)6 * 4 * 3 * n, 0);
   for (int f = 0; f < 6; ++f)
     for (int e = 0; e < 4; ++e) {
       const EdgeRoute rt = kRoutes[f][e];
       const int kind = rt.src_face < 4 ? 0 : rt.src_face - 3;
+      const size_t fe = (size_t)f * 4 + e;
       for (int l = 0; l < 3; ++l) {
         const int fixed = (rt.src_edge == kS || rt.src_edge == kW) ? l + 1 : n - 2 - l;
         for (int q = 0; q < n; ++q) {
           const int qs = rt.reversed ? n - 1 - q : q;
           const int s0 = t.s0[(size_t)l * n + qs];
+          t.s0t[(fe * 3 + l) * n + q] = s0;
           const double c0 = ROT(rt.src_face, rt.src_edge, l, qs, 0);
           const double c1 = ROT(rt.src_face, rt.src_edge, l, qs, 1);
           for (int s = 0; s < 9; ++s) {
@@ -281,11 +283,10 @@ int build_tables(const solar_desc& d, HostTables& t, std::string& err) {
             const size_t p2 = (size_t)jj * n + ii;
             const double w = t.w9[((size_t)l * n + qs) * 9 + s];
             const double* a = &t.conv[(size_t)kind * 4 * P2];
-            const size_t row = ((((size_t)f * 4 + e) * 3 + l) * n + q) * 9 + s;
-            t.ew[row] = w;
-            t.esrc[row] = (int)p2;
-            t.eg[row * 2 + 0] = w * (c0 * a[0 * P2 + p2] + c1 * a[2 * P2 + p2]);
-            t.eg[row * 2 + 1] = w * (c0 * a[1 * P2 + p2] + c1 * a[3 * P2 + p2]);
+            const size_t row = (fe * 3 + l) * 9 + s;
+            t.ew[row * n + q] = w;
+            t.eg[(row * 2 + 0) * n + q] = w * (c0 * a[0 * P2 + p2] + c1 * a[2 * P2 + p2]);
+            t.eg[(row * 2 + 1) * n + q] = w * (c0 * a[1 * P2 + p2] + c1 * a[3 * P2 + p2]);
           }
         }
       }

@@ -72,13 +72,15 @@ struct HostTables {
   std::vector<int> s0;                             // [3 layers][n] window start
   std::vector<double> interpolant;                 // [3][n][9] reference layout (iter+4)
   std::vector<double> rot;                         // [6][4][3][n][2] receiver-frame (cth, cph)
-  // Folded edge coefficients, indexed by the RECEIVING face / edge:
-  //   scalar ghost  = sum_s ew[f][e][l][t][s] * f(src point s)
-  //   vector ghost  = sum_s eg[f][e][l][t][s][0] * v_xi(src s) + eg[...][1] * v_eta(src s)
-  // (Lagrange weight x local->global conversion at the source point x receiver rotation)
-  std::vector<double> ew;                          // [6][4][3][n][9]
-  std::vector<double> eg;                          // [6][4][3][n][9][2]
-  std::vector<int> esrc;                           // [6][4][3][n][9] source point (j*n + i)
+  // Folded edge coefficients, indexed by the RECEIVING face / edge and stored with the
+  // position along the edge fastest (t):
+  //   scalar ghost  = sum_s ew[f][e][l][s][t] * f(source tap s)
+  //   vector ghost  = sum_s eg[f][e][l][s][0][t] * v_xi(tap s) + eg[f][e][l][s][1][t] * v_eta(tap s)
+  // (Lagrange weight x local->global conversion at the source point x receiver rotation);
+  // tap s sits at position s0t[f][e][l][t] + s of the source line.
+  std::vector<double> ew;                          // [6][4][3][9][n]
+  std::vector<double> eg;                          // [6][4][3][9][2][n]
+  std::vector<int> s0t;                            // [6][4][3][n]
   std::vector<double> dr_weight;                   // [nr] radial volume weight r^2 dr
 };
 
