@@ -146,6 +146,10 @@ int solar_gpu_last_error(char* buf, int len);
 /* ABI version (SOLAR_GPU_ABI_VERSION). */
 int solar_gpu_abi_version(void);
 
+/* Name of CUDA device `device` (NUL-terminated, truncated to len); used to key tuned
+ * launch shapes.  No counterpart in the reference (it has no device). */
+int solar_gpu_device_name(int device, char* buf, int len);
+
 #ifdef __cplusplus
 }
 #endif

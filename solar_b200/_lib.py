@@ -61,6 +61,7 @@ EXPORTS = {
     "solar_gpu_synchronize": [_P],
     "solar_gpu_last_error": [ctypes.c_char_p, ctypes.c_int],
     "solar_gpu_abi_version": [],
+    "solar_gpu_device_name": [ctypes.c_int, ctypes.c_char_p, ctypes.c_int],
 }
 
 _lib = None
@@ -88,6 +89,13 @@ def load(build_if_missing: bool = False):
         fn.restype = None if name == "solar_desc_defaults" else ctypes.c_int
     _lib = lib
     return lib
+
+
+def device_name(device: int = 0) -> str:
+    buf = ctypes.create_string_buffer(256)
+    if load().solar_gpu_device_name(device, buf, 256) != SOLAR_OK:
+        return "unknown"
+    return buf.value.decode(errors="replace")
 
 
 def last_error() -> str:

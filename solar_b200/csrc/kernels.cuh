@@ -79,6 +79,31 @@ template <> struct Coef<float> {
   __device__ static float filtr(int m) { return cFiltRF[m]; }
 };
 
+__host__ __device__ constexpr size_t align128(size_t b) { return (b + 127) / 128 * 128; }
+
+// 16-byte vectors: V = 4 floats or 2 doubles.
+template <typename T> struct Vec16;
+template <> struct Vec16<float> { using type = float4; static constexpr int V = 4; };
+template <> struct Vec16<double> { using type = double2; static constexpr int V = 2; };
+
+template <typename T>
+__device__ __forceinline__ void ldv(const T* p, T* out) {
+  using VT = typename Vec16<T>::type;
+  const VT v = *reinterpret_cast<const VT*>(p);
+  const T* e = reinterpret_cast<const T*>(&v);
+#pragma unroll
+  for (int q = 0; q < Vec16<T>::V; ++q) out[q] = e[q];
+}
+template <typename T>
+__device__ __forceinline__ void stv(T* p, const T* in) {
+  using VT = typename Vec16<T>::type;
+  VT v;
+  T* e = reinterpret_cast<T*>(&v);
+#pragma unroll
+  for (int q = 0; q < Vec16<T>::V; ++q) e[q] = in[q];
+  *reinterpret_cast<VT*>(p) = v;
+}
+
 // ---------------------------------------------------------------------------------
 // Edge (ghost) kernel: INTERPOLATE_ALONG_X/Y + TRANSFORM_VECTOR_BETWEEN_MESHES_DIV + the
 // inter-zone exchange and its reversal, in one pass.  Every ghost value is a 9-tap sum
@@ -146,63 +171,93 @@ __global__ void __launch_bounds__(128) edge_kernel(const EdgeArgs<T> a) {
   cp_async_wait_all();
   __syncthreads();
   const long long fstr = (long long)KC * 3 * n;         // field stride inside buf
-  for (int pr = threadIdx.x; pr < 3 * n; pr += blockDim.x) {
-    const int l = pr / n, t = pr - l * n;               // receiver layer and position
-    const long long crow = ((long long)fe * 3 + l) * 9;  // tap rows of this (face, edge, layer)
-    const int s0 = a.s0t[((long long)fe * 3 + l) * n + t];
-    long long dst;
-    if (e == 0) dst = g.at(0, -1 - l, t);
-    else if (e == 1) dst = g.at(0, n + l, t);
-    else if (e == 2) dst = g.at(0, t, -1 - l);
-    else dst = g.at(0, t, n + l);
-    T w[9];
+  // W/E receivers write their three ghost columns of a row as one whole 32-byte sector
+  // (ghost layers plus the unused padding columns next to them); writing 12 of 32 bytes
+  // would make the L2 read the sector back from DRAM to merge it.
+  const bool cols = e >= 2;
+  constexpr int SECT = 32 / sizeof(T);                   // elements per 32-byte sector
+  const int npairs = cols ? n : 3 * n;
+  for (int pr = threadIdx.x; pr < npairs; pr += blockDim.x) {
+    const int t = cols ? pr : pr % n;
+    const int lfirst = cols ? 0 : pr / n, lcount = cols ? 3 : 1;
+    // write the planes of one field: rows for S/N receivers, one sector per row for W/E
+    auto put = [&](T* base, const T (&res)[3][KC]) {
 #pragma unroll
-    for (int s = 0; s < 9; ++s) w[s] = a.ew[(crow + s) * n + t];
-    const int b0 = l * n + s0;
+      for (int kk = 0; kk < KC; ++kk) {
+        if (kk >= kc) continue;
+        if (!cols) {
+          base[(long long)kk * g.plane + g.at(0, e == 0 ? -1 - lfirst : n + lfirst, t)] = res[0][kk];
+        } else {
+          T sect[SECT];
+#pragma unroll
+          for (int m = 0; m < SECT; ++m) sect[m] = T(0);
+#pragma unroll
+          for (int l = 0; l < 3; ++l) sect[e == 2 ? SECT - 1 - l : l] = res[l][kk];
+          T* d = base + (long long)kk * g.plane + g.at(0, t, e == 2 ? -SECT : n);
+          stv(d, sect);
+          stv(d + Vec16<T>::V, sect + Vec16<T>::V);
+        }
+      }
+    };
     if (a.mode == 1) {
       for (int f = 0; f < nfl; ++f) {
-        T* out = a.q + g.vol(run, face, slot_of(f)) + (long long)kb * g.plane + dst;
-        const T* bf = buf + f * fstr + b0;
+        T res[3][KC];
+        for (int li = 0; li < lcount; ++li) {
+          const int l = lfirst + li;
+          const long long crow = ((long long)fe * 3 + l) * 9;
+          const T* b0 = buf + f * fstr + l * n + a.s0t[((long long)fe * 3 + l) * n + t];
+          T w[9];
 #pragma unroll
-        for (int kk = 0; kk < KC; ++kk) {
-          if (kk < kc) {
-            const T* b = bf + kk * 3 * n;
+          for (int s = 0; s < 9; ++s) w[s] = a.ew[(crow + s) * n + t];
+#pragma unroll
+          for (int kk = 0; kk < KC; ++kk) {
+            const T* b = b0 + kk * 3 * n;
             T a0 = T(0), a1 = T(0);
+            if (kk < kc) {
 #pragma unroll
-            for (int s = 0; s < 9; s += 2) a0 = fma(w[s], b[s], a0);
+              for (int s = 0; s < 9; s += 2) a0 = fma(w[s], b[s], a0);
 #pragma unroll
-            for (int s = 1; s < 9; s += 2) a1 = fma(w[s], b[s], a1);
-            out[(long long)kk * g.plane] = a0 + a1;
+              for (int s = 1; s < 9; s += 2) a1 = fma(w[s], b[s], a1);
+            }
+            res[li][kk] = a0 + a1;
           }
         }
+        put(a.q + g.vol(run, face, slot_of(f)) + (long long)kb * g.plane, res);
       }
       continue;
     }
-    T gx[9], gy[9];
+    T res_p[3][KC], res_v[3][KC];
+    for (int li = 0; li < lcount; ++li) {
+      const int l = lfirst + li;
+      const long long crow = ((long long)fe * 3 + l) * 9;
+      const int b0 = l * n + a.s0t[((long long)fe * 3 + l) * n + t];
+      T w[9], gx[9], gy[9];
 #pragma unroll
-    for (int s = 0; s < 9; ++s) {
-      gx[s] = a.eg[((crow + s) * 2 + 0) * n + t];
-      gy[s] = a.eg[((crow + s) * 2 + 1) * n + t];
-    }
-    T* op = a.q + g.vol(run, face, g.slot[kP]) + (long long)kb * g.plane + dst;
-    T* ov = a.q + g.vol(run, face, (e >= 2) ? g.slot[kVxi] : g.slot[kVeta]) + (long long)kb * g.plane + dst;
+      for (int s = 0; s < 9; ++s) {
+        w[s] = a.ew[(crow + s) * n + t];
+        gx[s] = a.eg[((crow + s) * 2 + 0) * n + t];
+        gy[s] = a.eg[((crow + s) * 2 + 1) * n + t];
+      }
 #pragma unroll
-    for (int kk = 0; kk < KC; ++kk) {
-      if (kk < kc) {
-        const T* bp = buf + b0 + kk * 3 * n;
-        const T* bx = bp + fstr;
-        const T* by = bx + fstr;
+      for (int kk = 0; kk < KC; ++kk) {
         T ap = T(0), ax = T(0), ay = T(0);
+        if (kk < kc) {
+          const T* bp = buf + b0 + kk * 3 * n;
+          const T* bx = bp + fstr;
+          const T* by = bx + fstr;
 #pragma unroll
-        for (int s = 0; s < 9; ++s) {
-          ap = fma(w[s], bp[s], ap);
-          ax = fma(gx[s], bx[s], ax);
-          ay = fma(gy[s], by[s], ay);
+          for (int s = 0; s < 9; ++s) {
+            ap = fma(w[s], bp[s], ap);
+            ax = fma(gx[s], bx[s], ax);
+            ay = fma(gy[s], by[s], ay);
+          }
         }
-        op[(long long)kk * g.plane] = ap;
-        ov[(long long)kk * g.plane] = ax + ay;
+        res_p[li][kk] = ap;
+        res_v[li][kk] = ax + ay;
       }
     }
+    put(a.q + g.vol(run, face, g.slot[kP]) + (long long)kb * g.plane, res_p);
+    put(a.q + g.vol(run, face, cols ? g.slot[kVxi] : g.slot[kVeta]) + (long long)kb * g.plane, res_v);
   }
 }
 
@@ -230,7 +285,8 @@ enum { mD = 0, mXYD, mC, mXYC, mDivX, mDivY, mTX, mTY, mVol, mCount };
 // MODE 2: write the raw COMPUTE_RHS into qout.  MODE 3: write (grad_xi, grad_eta,
 // grad_r, div) into the v_xi, v_eta, v_r, p slots of qout.
 constexpr int kLead = 7;
-constexpr int kTile = 3;
+// tile-ring depth: plane k is computed while planes k+1, k+2 are in flight
+template <typename T> struct TileRing { static constexpr int value = 3; };
 
 template <typename T>
 struct StageArgs {
@@ -251,31 +307,6 @@ struct StageArgs {
   int kchunk;
 };
 
-__host__ __device__ constexpr size_t align128(size_t b) { return (b + 127) / 128 * 128; }
-
-// 16-byte vectors: V = 4 floats or 2 doubles.
-template <typename T> struct Vec16;
-template <> struct Vec16<float> { using type = float4; static constexpr int V = 4; };
-template <> struct Vec16<double> { using type = double2; static constexpr int V = 2; };
-
-template <typename T>
-__device__ __forceinline__ void ldv(const T* p, T* out) {
-  using VT = typename Vec16<T>::type;
-  const VT v = *reinterpret_cast<const VT*>(p);
-  const T* e = reinterpret_cast<const T*>(&v);
-#pragma unroll
-  for (int q = 0; q < Vec16<T>::V; ++q) out[q] = e[q];
-}
-template <typename T>
-__device__ __forceinline__ void stv(T* p, const T* in) {
-  using VT = typename Vec16<T>::type;
-  VT v;
-  T* e = reinterpret_cast<T*>(&v);
-#pragma unroll
-  for (int q = 0; q < Vec16<T>::V; ++q) e[q] = in[q];
-  *reinterpret_cast<VT*>(p) = v;
-}
-
 template <typename T, int TX, int TY, bool HAS_RHO>
 struct StageLayout {
   static constexpr int PB = (TX + 8) * (TY + 6), XB = (TX + 8) * TY, YB = TX * (TY + 6), OB = TX * TY;
@@ -286,8 +317,9 @@ struct StageLayout {
   static constexpr size_t O_BYTES = align128(OB * sizeof(T));
   static constexpr size_t LEAD = P_BYTES + O_BYTES;                    // p box + v_r
   static constexpr size_t TILE = X_BYTES + Y_BYTES + NO * O_BYTES;     // v_xi, v_eta, (rho), qw
-  static constexpr size_t BAR = kLead * LEAD + kTile * TILE;
-  static constexpr size_t TOTAL = BAR + (kLead + kTile) * sizeof(uint64_t);
+  static constexpr int RING = TileRing<T>::value;
+  static constexpr size_t BAR = kLead * LEAD + RING * TILE;
+  static constexpr size_t TOTAL = BAR + (kLead + RING) * sizeof(uint64_t);
 };
 
 // Each thread owns V consecutive points of one row (V = 16 bytes / sizeof(T)), so the
@@ -295,6 +327,7 @@ struct StageLayout {
 template <typename T, int TX, int TY, int MODE, bool HAS_RHO>
 __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __grid_constant__ StageArgs<T> a) {
   constexpr int V = Vec16<T>::V;
+  constexpr int kTile = TileRing<T>::value;
   constexpr int NT = TX / V;
   constexpr int NV = (V + 8) / V;            // vectors covering box columns c .. c+V+7
   constexpr int PW = TX + 8;
@@ -388,6 +421,23 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __
   const int yc = (ty + 3) * TX + V * cx;
   const int oc = ty * TX + V * cx;
 
+  // radial coefficients of the current plane; the next plane's are loaded one iteration
+  // ahead so their latency hides behind the compute
+  struct Rad { T facr, invr, rho0, inv_rho0, c2rho0, rho0g0, sig, drho0, g0rho0; };
+  auto load_rad = [&](int k) {
+    Rad r;
+    r.facr = __ldg(a.rad + rFacR * nr + k);
+    r.invr = __ldg(a.rad + rInvR * nr + k);
+    r.rho0 = __ldg(a.rad + rRho0 * nr + k);
+    r.inv_rho0 = __ldg(a.rad + rInvRho0 * nr + k);
+    r.c2rho0 = __ldg(a.rad + rC2Rho0 * nr + k);
+    r.rho0g0 = __ldg(a.rad + rRho0G0 * nr + k);
+    r.sig = __ldg(a.rad + rSigma * nr + k);
+    r.drho0 = HAS_RHO ? __ldg(a.rad + rDRho0 * nr + k) : T(0);
+    r.g0rho0 = HAS_RHO ? __ldg(a.rad + rG0Rho0 * nr + k) : T(0);
+    return r;
+  };
+  Rad rc = load_rad(kb);
   T pw[7][V], vw[7][V];
 #pragma unroll
   for (int s = 0; s < 7; ++s)
@@ -410,6 +460,7 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __
       if (++slot_q == kLead) { slot_q = 0; phase_q ^= 1; }
     }
     ok &= mbar_wait(&barT[slot_t], phase_t, a.err, 2);
+    const Rad rn = load_rad(min(k + 1, nr - 1));
     const T* sp = reinterpret_cast<const T*>(lead(slot_k));
     const unsigned char* tb = tile(slot_t);
     const T* sx = reinterpret_cast<const T*>(tb);
@@ -436,8 +487,8 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __
           const int sl = HAS_RHO ? f : f - 1;
           ldv(reinterpret_cast<const T*>(tb + L::X_BYTES + L::Y_BYTES + (QOFF + sl) * L::O_BYTES) + oc, qwv[f]);
         }
-    const T facr = __ldg(a.rad + rFacR * nr + k);
-    const T invr = __ldg(a.rad + rInvR * nr + k);
+    const T facr = rc.facr;
+    const T invr = rc.invr;
     const bool interior = k >= 3 && k <= nr - 4;
     const int offk = k - ks;
     const int brow = k < 3 ? k : nr - 1 - k;
@@ -477,16 +528,16 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __
       if (MODE == 3) {
         o0[q] = gxi; o1[q] = geta; o2[q] = dpr; o3[q] = div;
       } else {
-        const T rho0 = __ldg(a.rad + rRho0 * nr + k), inv_rho0 = __ldg(a.rad + rInvRho0 * nr + k);
-        T c2rho0 = __ldg(a.rad + rC2Rho0 * nr + k);
+        const T rho0 = rc.rho0, inv_rho0 = rc.inv_rho0;
+        T c2rho0 = rc.c2rho0;
         if (a.c2) c2rho0 = a.c2[((long long)face * nr + k) * P2 + p2 + q] * rho0;
         r_vx[q] = -gxi * inv_rho0;
         r_ve[q] = -geta * inv_rho0;
         r_vr[q] = -dpr * inv_rho0;
-        r_p[q] = -c2rho0 * div + __ldg(a.rad + rRho0G0 * nr + k) * v_r;
+        r_p[q] = -c2rho0 * div + rc.rho0g0 * v_r;
         if (HAS_RHO) {
-          r_rho[q] = -rho0 * div - v_r * __ldg(a.rad + rDRho0 * nr + k);
-          r_vr[q] -= rho[q] * __ldg(a.rad + rG0Rho0 * nr + k);
+          r_rho[q] = -rho0 * div - v_r * rc.drho0;
+          r_vr[q] -= rho[q] * rc.g0rho0;
         }
       }
     }
@@ -505,7 +556,7 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __
     } else {
       // BC_RHS (bc_acoustic_wave.f90:432-452) then SPONGE (sponge.f90:502-504)
       const bool bc = (k == 0 || k == nr - 1);
-      const T sig = __ldg(a.rad + rSigma * nr + k);
+      const T sig = rc.sig;
       const T dt = a.dt, alpha = a.alpha, beta = a.beta;
       // qw = alpha qw + dt rhs ; q = q + beta qw   (timestep.f90:68-69)
       auto update = [&](int f, const T* qv, const T* rv, bool damped) {
@@ -537,6 +588,7 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __
     }
     if (++slot_t == kTile) { slot_t = 0; phase_t ^= 1; }
     if (++slot_k == kLead) slot_k = 0;
+    rc = rn;
   }
   if (!ok && tid == 0) {
     // a wait gave up: give copies still in flight a bounded time to land before exit

@@ -441,6 +441,15 @@ void solar_desc_defaults(solar_desc* d) {
 
 int solar_gpu_abi_version(void) { return SOLAR_GPU_ABI_VERSION; }
 
+int solar_gpu_device_name(int device, char* buf, int len) {
+  if (!buf || len <= 0) return fail(SOLAR_ERR_ARG, "null buffer");
+  cudaDeviceProp p;
+  cudaError_t e = cudaGetDeviceProperties(&p, device);
+  if (e != cudaSuccess) return fail(SOLAR_ERR_CUDA, "cudaGetDeviceProperties: %s", cudaGetErrorString(e));
+  std::snprintf(buf, (size_t)len, "%s", p.name);
+  return SOLAR_OK;
+}
+
 int solar_gpu_last_error(char* buf, int len) {
   if (!buf || len <= 0) return SOLAR_ERR_ARG;
   std::snprintf(buf, (size_t)len, "%s", solar::g_last_error.c_str());
@@ -508,7 +517,7 @@ int solar_gpu_init(const solar_desc* d, solar_ctx** out) {
   if (d->kchunk > 0) c->kchunk = d->kchunk;
   else {
     const long long blocks = 6LL * g.nruns * (g.n / c->tile_x) * (g.n / c->tile_y);
-    const long long want = 148LL * 6;
+    const long long want = 148LL * 2 * 4;   // about four waves of two resident CTAs per SM
     int nch = (int)std::max<long long>(1, (want + blocks - 1) / blocks);
     c->kchunk = std::max(8, (g.nr + nch - 1) / nch);
   }

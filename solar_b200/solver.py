@@ -37,7 +37,8 @@ class Solver:
 
     def __init__(self, cfg: Config, precision: str = "fp64", nfields: int = 5, nruns: int = 1,
                  device: int = 0, fix_reversed_rotation: bool = False,
-                 c2_3d: Optional[np.ndarray] = None, tile: Optional[Sequence[int]] = None):
+                 c2_3d: Optional[np.ndarray] = None, tile: Optional[Sequence[int]] = None,
+                 tuned: bool = True):
         self.lib = _lib.load()
         self.cfg = cfg
         self.nx, self.nr = cfg.nx, cfg.nr
@@ -60,8 +61,12 @@ class Solver:
         d.sponge_amp, d.sponge_exp, d.sponge_len = float(sp.amp), float(sp.exp), int(sp.length)
         d.sponge_lower, d.sponge_upper = int(sp.lower), int(sp.upper)
         d.fix_reversed_rotation = int(bool(fix_reversed_rotation))
+        if tile is None and tuned:
+            from . import autotune
+            tile = autotune.lookup(cfg.nx, cfg.nr, precision, nfields, nruns, device)
         if tile is not None:
             d.tile_x, d.tile_y, d.kchunk = (list(tile) + [0, 0, 0])[:3]
+        self.tile = tile
         self.desc = d
         h = ctypes.c_void_p()
         _lib.check(self.lib.solar_gpu_init(ctypes.byref(d), ctypes.byref(h)))
