@@ -125,6 +125,18 @@ int solar_gpu_divergence(solar_ctx* c, const double* v_xi, const double* v_eta,
  * (sum(f^2) / (nx*ny*nr) * 6)^0.5 over the six zones, the reference's formula. */
 int solar_gpu_norm(solar_ctx* c, int run, int field, double* out);
 
+/* The same norm of a six-zone FP64 field f[zone][k][j][i] that already lives in device
+ * memory, for callers that cannot allocate (a host whose device memory is budgeted by
+ * another runtime, or a per-step diagnostic hook that must not trigger the device-wide
+ * synchronisation of cudaMalloc/cudaFree).  No counterpart in the reference: it has no
+ * device.  Allocates nothing: its scratch is a fixed 96 KiB device array inside the
+ * library, so nr <= 2048 (larger grids return SOLAR_ERR_ARG).  d_out is one device double;
+ * the call only enqueues work on `stream` (a cudaStream_t, NULL = legacy default stream).
+ * The first call on a device resolves the scratch address and should come before any
+ * stream capture.  Calls whose kernels overlap on the same device race on the shared
+ * scratch. */
+int solar_gpu_norm_noalloc(const double* d_field, int nx, int nr, double* d_out, void* stream);
+
 /* FP64 diagnostics of one run: out[0] = acoustic energy
  * 1/2 sum (rho0 |v|^2 + p^2 / (rho0 c^2)) dV, out[1] = sum rho dV, out[2] = max |p|,
  * out[3] = 1 if any value is NaN/Inf.  dV is the cubed-sphere volume element

@@ -16,8 +16,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsolar_gpu.so")
-SOURCES = [os.path.join(CSRC, "solar_gpu.cu"), os.path.join(CSRC, "tables.cpp")]
-HEADERS = [os.path.join(CSRC, "kernels.cuh"), os.path.join(CSRC, "tables.h"),
+SOURCES = [os.path.join(CSRC, "solar_gpu.cu"), os.path.join(CSRC, "noalloc.cu"), os.path.join(CSRC, "tables.cpp")]
+HEADERS = [os.path.join(CSRC, "kernels.cuh"), os.path.join(CSRC, "tma.cuh"), os.path.join(CSRC, "tables.h"),
            os.path.join(ROOT, "include", "solar_gpu.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

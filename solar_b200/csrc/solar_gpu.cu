@@ -29,6 +29,9 @@ static int fail(int code, const char* fmt, ...) {
   return code;
 }
 
+// Shared with the other translation units of the library.
+int report_error(int code, const char* msg) { return fail(code, "%s", msg); }
+
 #define CK(call)                                                                          \
   do {                                                                                    \
     cudaError_t e_ = (call);                                                              \
