@@ -40,6 +40,20 @@ sys.path.insert(0, ROOT)
 import numpy as np  # noqa: E402
 
 
+def stage_traffic(cfg, tile):
+    """DRAM bytes per stage launch (mean over the five stages of a step) from the committed
+    ncu launch-list summary, when it covers this workload; else None."""
+    import re
+    if cfg.name != "c2" or cfg.nx != 128:
+        return None
+    try:
+        txt = open(os.path.join(ROOT, "profiles", "launch_list_c2_6x128cubed.md")).read()
+        m = re.search(r"traffic_stage_fp32_mean_bytes_per_launch = (\d+)", txt)
+        return float(m.group(1)) if m else None
+    except Exception:
+        return None
+
+
 def load_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -211,6 +225,7 @@ def main():
 
     # ---------------------------------------------------------------- FP32 fused path
     s32 = Solver(cfg, precision="fp32", nfields=4, device=local)
+    tile32 = list(s32.tile) if s32.tile else "default"
     s32.init_sources()
     s32.rk4(args.warmup)
     barrier(world)
@@ -293,8 +308,9 @@ def main():
                  "stage_ms": kt64["stage_ms"], "filter_ms": kt64["filter_ms"], "edge_ms": kt64["edge_ms"]},
         "fp32_rel_err_vs_fp64": err,
         "roofline": {"bound": "hbm", "achieved": stage_gbs, "peak": peak, "unit": "GB/s",
-                     "frac": stage_gbs / peak, "traffic": None, "peak_kind": peak_kind,
-                     "kernel": "stage_kernel<float,32,8>", "algorithmic_bytes_per_launch": stage_bytes,
+                     "frac": stage_gbs / peak, "traffic": stage_traffic(cfg, tile32), "peak_kind": peak_kind,
+                     "kernel": "stage_kernel<float> (tile x, tile y, planes per CTA = %s)" % (tile32,),
+                     "algorithmic_bytes_per_launch": stage_bytes,
                      "mean_launch_ms": kt["stage_ms"],
                      "filter": {"achieved": filter_gbs, "frac": filter_gbs / peak, "mean_launch_ms": kt["filter_ms"]},
                      "edge_mean_launch_ms": kt["edge_ms"],
