@@ -152,6 +152,44 @@ int solar_gpu_time_rk4(solar_ctx* c, int nsteps, int per_kernel, double* out7);
 /* Block until the context's stream is idle. */
 int solar_gpu_synchronize(solar_ctx* c);
 
+/* ---- Discrete adjoint (run 0 of a context with nruns == 1) -------------------------
+ * No counterpart in the reference, which has no adjoint.  These are the exact transposes
+ * of the discrete forward operators above: COMPUTE_RHS + BC_RHS + SPONGE, FILTER_EXP
+ * (with the halo interpolation and vector rotation of the edge exchange) and the 2N-RK
+ * step of timestep.f90:61-82 run backwards stage by stage.  Host arrays use the
+ * six-zone Fortran order of the header comment.
+ *
+ * Receivers sample p with trilinear weights on one face: loc[4*r .. 4*r+3] =
+ * (zone 0..5, i, j, k) as fractional 0-based grid indices (i along xi, j along eta,
+ * k along the radius), each inside [0, nx-1] x [0, nx-1] x [0, nr-1]. */
+int solar_gpu_set_receivers(solar_ctx* c, int nrec, const double* loc);
+
+/* nsteps forward steps from the current state; traces[n*nrec + r] = p at receiver r
+ * after step n+1.  Leaves the state at step nsteps. */
+int solar_gpu_record(solar_ctx* c, int nsteps, double* traces);
+
+/* Misfit J = 1/2 sum_{n=1..nsteps} sum_r (p_r(t_n) - data[(n-1)*nrec + r])^2 of an
+ * nsteps-step run from the current state, and its gradient with respect to the sound
+ * speed c at every grid point: grad_c[zone][k][j][i] = dJ/dc (0 on the two radial
+ * boundary planes, where BC_RHS discards the right-hand side).  The state is
+ * checkpointed every `checkpoint_every` steps; each segment is recomputed once during
+ * the reverse sweep, storing the divergence of its stage inputs (memory: one state per
+ * checkpoint plus 5 * checkpoint_every field volumes).  Optional outputs (may be NULL):
+ * misfit, grad_c, lambda0 = dJ/dq at the initial state (state array), times_ms[3] =
+ * device time of the forward sweep, the recomputation and the reverse sweep.  On
+ * return the state is back at the initial condition. */
+int solar_gpu_misfit_gradient(solar_ctx* c, int nsteps, int checkpoint_every, const double* data,
+                              double* misfit, double* grad_c, double* lambda0, double* times_ms);
+
+/* out = L^T mu, L(q) = SPONGE(BC_RHS(COMPUTE_RHS(q))) as a linear map of the state. */
+int solar_gpu_rhs_adjoint(solar_ctx* c, const double* mu, double* out);
+
+/* out = FILTER_EXP^T lam (halo interpolation included). */
+int solar_gpu_filter_adjoint(solar_ctx* c, const double* lam, double* out);
+
+/* lam_out = (STEP^T)^nsteps lam_in, STEP = one RK4 call (five stages + FILTER_EXP). */
+int solar_gpu_rk4_adjoint(solar_ctx* c, int nsteps, const double* lam_in, double* lam_out);
+
 /* Copy the last error message of this thread (NUL-terminated, truncated to len). */
 int solar_gpu_last_error(char* buf, int len);
 

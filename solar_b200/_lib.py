@@ -14,6 +14,12 @@ _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int)
 
 SOLAR_OK = 0
+SOLAR_ERR_ARG = -1
+SOLAR_ERR_CUDA = -2
+SOLAR_ERR_NAN = -3
+SOLAR_ERR_TIMEOUT = -4
+SOLAR_ERR_STATE = -5
+SOLAR_ERR_NOMEM = -6
 SOLAR_FP64 = 0
 SOLAR_FP32 = 1
 
@@ -63,6 +69,12 @@ EXPORTS = {
     "solar_gpu_last_error": [ctypes.c_char_p, ctypes.c_int],
     "solar_gpu_abi_version": [],
     "solar_gpu_device_name": [ctypes.c_int, ctypes.c_char_p, ctypes.c_int],
+    "solar_gpu_set_receivers": [_P, ctypes.c_int, _D],
+    "solar_gpu_record": [_P, ctypes.c_int, _D],
+    "solar_gpu_misfit_gradient": [_P, ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _D],
+    "solar_gpu_rhs_adjoint": [_P, _D, _D],
+    "solar_gpu_filter_adjoint": [_P, _D, _D],
+    "solar_gpu_rk4_adjoint": [_P, ctypes.c_int, _D, _D],
 }
 
 _lib = None

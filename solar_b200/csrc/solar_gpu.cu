@@ -56,6 +56,25 @@ struct DevTables {
   double* gr = nullptr;    // [nr]
 };
 
+// Device arrays of the discrete adjoint, allocated on first use (nruns == 1 only).
+struct AdjBuffers {
+  void* L = nullptr;        // lambda_q (padded state layout; frames hold ghost adjoints)
+  void* LW = nullptr;       // lambda_w
+  void* T1 = nullptr;       // filter-transpose scratch
+  void* T2 = nullptr;
+  void* I = nullptr;        // six intermediate volumes per face
+  double* grad = nullptr;   // dJ/dc, compact [face][k][j][i]
+  void* ckpt = nullptr;     // state checkpoints (padded copies of the state buffer)
+  size_t ckpt_bytes = 0;
+  void* div = nullptr;      // stage-input divergences of one checkpoint segment
+  size_t div_bytes = 0;
+  double* traces = nullptr; // receiver traces and residuals
+  size_t traces_bytes = 0;
+  long long* rec_off = nullptr;
+  double* rec_w = nullptr;
+  int nrec = 0;
+};
+
 }  // namespace solar
 
 using namespace solar;
@@ -83,6 +102,7 @@ struct solar_ctx {
   cudaGraphExec_t step_graph = nullptr;
   cudaGraphExec_t batch_graph = nullptr;
   cudaEvent_t ev[8] = {};
+  AdjBuffers adj;
 };
 
 namespace solar {
@@ -470,6 +490,10 @@ int solar_gpu_finalize(solar_ctx* c) {
                   c->dt.rad64, c->dt.vol2, c->dt.drw, c->dt.c2_64, c->dt.tanx, c->dt.gr};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  void* aptrs[] = {c->adj.L, c->adj.LW, c->adj.T1, c->adj.T2, c->adj.I, c->adj.grad, c->adj.ckpt,
+                   c->adj.div, c->adj.traces, c->adj.rec_off, c->adj.rec_w};
+  for (void* p : aptrs)
+    if (p) cudaFree(p);
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -813,3 +837,5 @@ int solar_gpu_synchronize(solar_ctx* c) {
 }
 
 }  // extern "C"
+
+#include "adjoint_host.cuh"

@@ -192,3 +192,53 @@ class Solver:
 
     def synchronize(self) -> None:
         _lib.check(self.lib.solar_gpu_synchronize(self._h))
+
+    # ------------------------------------------------------------------ adjoint
+    def set_receivers(self, loc) -> None:
+        """Receivers as rows (zone 0..5, i, j, k) of fractional 0-based grid indices."""
+        loc = np.ascontiguousarray(loc, dtype=np.float64).reshape(-1, 4)
+        self.nrec = loc.shape[0]
+        _lib.check(self.lib.solar_gpu_set_receivers(self._h, self.nrec, _ptr(loc)))
+
+    def record(self, nsteps: int) -> np.ndarray:
+        """Run nsteps and return p at the receivers after every step, shape (nsteps, nrec)."""
+        out = np.empty((int(nsteps), self.nrec))
+        _lib.check(self.lib.solar_gpu_record(self._h, int(nsteps), _ptr(out)))
+        return out
+
+    def misfit_gradient(self, nsteps: int, checkpoint_every: int, data: np.ndarray,
+                        want_lambda: bool = False) -> dict:
+        """Misfit of the receiver traces against ``data`` (nsteps, nrec) and dJ/dc per point."""
+        data = np.ascontiguousarray(data, dtype=np.float64)
+        if data.shape != (int(nsteps), self.nrec):
+            raise ValueError(f"data must have shape {(int(nsteps), self.nrec)}")
+        J = ctypes.c_double()
+        grad = np.empty(self.field_shape)
+        lam = np.empty(self.state_shape) if want_lambda else None
+        times = (ctypes.c_double * 3)()
+        _lib.check(self.lib.solar_gpu_misfit_gradient(
+            self._h, int(nsteps), int(checkpoint_every), _ptr(data), ctypes.byref(J), _ptr(grad),
+            _ptr(lam) if lam is not None else None, times))
+        out = {"misfit": J.value, "grad_c": grad,
+               "forward_ms": times[0], "recompute_ms": times[1], "adjoint_ms": times[2]}
+        if lam is not None:
+            out["lambda0"] = lam
+        return out
+
+    def rhs_adjoint(self, mu: np.ndarray) -> np.ndarray:
+        mu = np.ascontiguousarray(mu, dtype=np.float64)
+        out = np.empty(self.state_shape)
+        _lib.check(self.lib.solar_gpu_rhs_adjoint(self._h, _ptr(mu), _ptr(out)))
+        return out
+
+    def filter_adjoint(self, lam: np.ndarray) -> np.ndarray:
+        lam = np.ascontiguousarray(lam, dtype=np.float64)
+        out = np.empty(self.state_shape)
+        _lib.check(self.lib.solar_gpu_filter_adjoint(self._h, _ptr(lam), _ptr(out)))
+        return out
+
+    def rk4_adjoint(self, nsteps: int, lam: np.ndarray) -> np.ndarray:
+        lam = np.ascontiguousarray(lam, dtype=np.float64)
+        out = np.empty(self.state_shape)
+        _lib.check(self.lib.solar_gpu_rk4_adjoint(self._h, int(nsteps), _ptr(lam), _ptr(out)))
+        return out
