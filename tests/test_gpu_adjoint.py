@@ -114,8 +114,8 @@ def adjoint_gradient(cfg, c, q0, loc, data, nsteps, k, precision="fp64", nfields
 
 def interior_direction(cfg, seed, smooth=False):
     rng = np.random.default_rng(seed)
-    if smooth:
-        centre = configs.unit_vectors(rng, 1)[0] * 0.8
+    if smooth:     # a blob in the region the receivers are sensitive to
+        centre = np.asarray(cfg.sources[0].x0) * 0.95 + rng.uniform(-0.05, 0.05, 3)
         d = receivers.sound_speed(cfg, [(tuple(centre), 0.1, 1.0)]) - receivers.sound_speed(cfg)
     else:
         d = rng.standard_normal((6, cfg.nr, cfg.nx, cfg.nx)) * receivers.sound_speed(cfg)
