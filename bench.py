@@ -199,6 +199,114 @@ def rel_errors(a, b, fields):
     return {names[m]: float(np.linalg.norm(a[:, m] - b[:, m]) / max(np.linalg.norm(b[:, m]), 1e-300)) for m in fields}
 
 
+def adjoint_block(device: int, nsteps: int, k: int, nfd: int):
+    """Misfit gradient dJ/dc on the adjoint workload (6 x 96^3 stratified shell, 32 receivers
+    at r = 0.98, data from a model with eight sound-speed anomalies), timed on the device,
+    and checked against central finite differences of the GPU FP64 misfit along nfd
+    directions (half random per point, half smooth blobs near the anomalies)."""
+    import numpy as np
+    from solar_b200 import configs, receivers
+    from solar_b200.solver import Solver
+
+    cfg = configs.c4(nsteps=nsteps)
+    loc = receivers.locate(cfg, cfg.receivers)
+    c0 = receivers.sound_speed(cfg)
+    c_true = receivers.sound_speed(cfg, cfg.dc_blobs)
+    with Solver(cfg, device=device) as s:
+        s.init_sources()
+        q0 = s.get_state()
+
+    def traces(c):
+        with Solver(cfg, device=device, c2_3d=c ** 2) as s:
+            s.set_state(q0)
+            s.set_receivers(loc)
+            return s.record(nsteps)
+
+    data = traces(c_true)
+    with Solver(cfg, device=device, c2_3d=c0 ** 2) as s:
+        s.set_state(q0)
+        s.set_receivers(loc)
+        s.misfit_gradient(min(k, nsteps), k, data[:min(k, nsteps)])      # warm-up, allocates
+        res = s.misfit_gradient(nsteps, k, data)
+    grad = res["grad_c"]
+    total_ms = res["forward_ms"] + res["recompute_ms"] + res["adjoint_ms"]
+    rng = np.random.default_rng(44)
+    errs = []
+    for m in range(nfd):
+        if m % 2 == 0:
+            d = rng.standard_normal(c0.shape) * c0
+        else:      # four blobs around the anomalies, where the receivers are sensitive
+            centres = np.array([cfg.dc_blobs[i][0] for i in rng.choice(len(cfg.dc_blobs), 4, replace=False)])
+            centres = centres + rng.uniform(-0.05, 0.05, centres.shape)
+            d = receivers.sound_speed(cfg, [(tuple(x), 0.06, 1.0) for x in centres]) - c0
+        d[:, 0] = 0.0
+        d[:, -1] = 0.0
+        eps = 1e-6 / np.abs(d / c0).max()
+        jp = 0.5 * float(((traces(c0 + eps * d) - data) ** 2).sum())
+        jm = 0.5 * float(((traces(c0 - eps * d) - data) ** 2).sum())
+        fd = (jp - jm) / (2 * eps)
+        ad = float(np.vdot(grad.ravel(), d.ravel()))
+        errs.append(abs(fd - ad) / abs(ad))
+    pts = cfg.points
+    return {
+        "workload": "c4: 6 x %d^3 stratified shell, %d steps, %d receivers, checkpoint every %d steps, FP64" % (
+            cfg.nx, nsteps, len(loc), k),
+        "misfit": res["misfit"], "gradient_ms": total_ms,
+        "forward_ms": res["forward_ms"], "recompute_ms": res["recompute_ms"], "adjoint_ms": res["adjoint_ms"],
+        "adjoint_pt_steps_per_s": pts * nsteps / (res["adjoint_ms"] / 1e3),
+        "gradient_cost_in_forward_runs": total_ms / res["forward_ms"],
+        "fd_directions": nfd, "fd_rel_err_max": max(errs) if errs else None,
+        "fd_rel_errs": errs, "fd_tolerance": 1e-4,
+    }
+
+
+def batch_block(device: int):
+    """The batched-sources workload: 64 independent runs of 6 x 64^3 (stratified shell,
+    per-run seeded source), uneven step counts 200..1000, FP32, all runs in the same
+    launches (one captured graph per step, finished runs masked off on the device)."""
+    from solar_b200 import configs
+    from solar_b200.solver import Solver
+
+    cfg = configs.c3()
+    R = len(cfg.runs)
+    with Solver(cfg, precision="fp32", nfields=4, nruns=R, device=device) as s:
+        for r in range(R):
+            s.init_sources(cfg.runs[r], run=r)
+        s.rk4_runs([3] * R)                                   # warm-up (graph capture)
+        ms = s.time_rk4_runs(cfg.run_steps)
+        tile = list(s.tile) if s.tile else "default"
+    work = cfg.points * sum(cfg.run_steps)
+    with Solver(cfg, precision="fp32", nfields=4, nruns=1, device=device) as s1:
+        s1.init_sources(cfg.runs[0])
+        s1.rk4(3)
+        one = s1.time_rk4(200)["total_ms"]
+    single = cfg.points * 200 / (one / 1e3)
+    return {"workload": "c3: %d runs of 6 x %d^3, steps %d..%d (sum %d), FP32 F=4" % (
+                R, cfg.nx, min(cfg.run_steps), max(cfg.run_steps), sum(cfg.run_steps)),
+            "value": work / (ms / 1e3), "unit": "grid-pt RK4 updates/s", "ms": ms,
+            "graph_replays": max(cfg.run_steps), "tile": tile,
+            "single_run_value": single, "batch_speedup_vs_one_run_at_a_time": (work / (ms / 1e3)) / single}
+
+
+def large_block(device: int, nsteps: int):
+    """The large-grid workload: 6 x 384^3 stratified shell, 16 sources, FP32 F=4 and FP64
+    F=5 on the same grid (state 5.7 GB / 14.4 GB per buffer)."""
+    from solar_b200 import configs
+    from solar_b200.solver import Solver
+
+    cfg = configs.c5(nsteps=nsteps)
+    out = {"workload": "c5: 6 x %d^3, %d steps" % (cfg.nx, nsteps)}
+    for prec, nf in (("fp32", 4), ("fp64", 5)):
+        with Solver(cfg, precision=prec, nfields=nf, device=device) as s:
+            s.init_sources()
+            s.rk4(3)
+            t = s.time_rk4(nsteps)
+            out[prec] = {"value": cfg.points * nsteps / (t["total_ms"] / 1e3), "ms_per_step": t["total_ms"] / nsteps,
+                         "fields": nf, "norm_vr": s.norm(4)}
+    out["fp32_speedup"] = out["fp32"]["value"] / out["fp64"]["value"]
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -208,6 +316,13 @@ def main():
     ap.add_argument("--config", default="c2")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adjoint-steps", type=int, default=500)
+    ap.add_argument("--adjoint-checkpoint", type=int, default=50)
+    ap.add_argument("--adjoint-fd", type=int, default=4)
+    ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-large", action="store_true")
+    ap.add_argument("--large-steps", type=int, default=200)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -290,6 +405,13 @@ def main():
 
     if rank != 0:
         return
+    adjoint = batch = large = None
+    if world == 1 and not args.no_adjoint:
+        adjoint = adjoint_block(local, args.adjoint_steps, args.adjoint_checkpoint, args.adjoint_fd)
+    if world == 1 and not args.no_batch:
+        batch = batch_block(local)
+    if world == 1 and not args.no_large:
+        large = large_block(local, args.large_steps)
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(cfg, 2)
@@ -320,6 +442,9 @@ def main():
         "clocks": clocks,
         "e2e": e2e,
         "cpu_baseline": cpu,
+        "adjoint": adjoint,
+        "batched_sources": batch,
+        "large_grid": large,
     }
     print(json.dumps(line), flush=True)
 

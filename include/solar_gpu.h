@@ -105,6 +105,10 @@ int solar_gpu_rk4(solar_ctx* c, int nsteps);
  * same launches, replayed from one captured CUDA graph. */
 int solar_gpu_rk4_runs(solar_ctx* c, const int* nsteps_per_run);
 
+/* solar_gpu_rk4_runs, plus the device time of the whole batch (CUDA events on the
+ * context's stream) in *ms. */
+int solar_gpu_time_rk4_runs(solar_ctx* c, const int* nsteps_per_run, double* ms);
+
 /* Operator-level drop-ins (host arrays in, host arrays out; use run 0's buffers):
  *   COMPUTE_RHS (compute_rhs_acoustic.f90:1-159, forcing off)        q -> rhs
  *   BC_RHS      (bc_acoustic_wave.f90:1-36)                          rhs in place

@@ -55,6 +55,7 @@ EXPORTS = {
     "solar_gpu_add_gaussian": [_P, ctypes.c_int] + [ctypes.c_double] * 5,
     "solar_gpu_rk4": [_P, ctypes.c_int],
     "solar_gpu_rk4_runs": [_P, _I],
+    "solar_gpu_time_rk4_runs": [_P, _I, _D],
     "solar_gpu_compute_rhs": [_P, _D, _D],
     "solar_gpu_bc_rhs": [_P, _D],
     "solar_gpu_sponge": [_P, _D, _D],

@@ -16,8 +16,11 @@ parameters with the shapes the workloads call for:
   one pulse of width 0.02 at r = 0.95 in a seeded uniform direction; 1000 steps.
 * ``c3``  64 independent runs on 6 x 64^3 with the c2 background, per-run seeded
   direction, width U[0.01, 0.03], amplitude U[0.5, 2], steps U{200..1000}.
-* ``c4``  6 x 96^3 c2 background plus a seeded sound-speed perturbation (eight
-  Gaussian blobs of width 0.03, total amplitude 0.01) and 32 receivers.
+* ``c4``  6 x 96^3 c2 background, one pulse (width 0.02) at r = 0.95, a seeded
+  sound-speed perturbation (eight Gaussian blobs of width 0.03, relative amplitude
+  0.01, between the source and the receivers) and 32 receivers at r = 0.98 within
+  0.05-0.25 rad of the source direction (the distance sound travels near r = 0.95
+  in 500 steps is about 0.3), 500 steps.
 * ``c5``  6 x 384^3 c2 background, 16 seeded sources, 200 steps.
 
 The time step follows a CFL of 0.5 (the reference overrides its own CFL estimate
@@ -189,19 +192,28 @@ def c3(nx: int = 64, nruns: int = 64, smin: int = 200, smax: int = 1000) -> Conf
 def c4(nx: int = 96, nsteps: int = 500, receiver_r: float = 0.98) -> Config:
     """Adjoint workload.  Receivers sit at r = 0.98: the reference filter zeroes the
     five outermost radial planes every step (filter.f90:726-775), which at nr = 96
-    covers r >= 0.987, so receivers at r = 0.99 would read p = 0."""
+    covers r >= 0.987, so receivers at r = 0.99 would read p = 0.  Receivers and
+    anomalies lie within reach of the pulse in 500 steps."""
     nr = nx
     model = model_stratified(nr)
     rng = np.random.default_rng(4)
-    # blob centres uniform in the shell volume (r^3 uniform)
-    dirs = unit_vectors(rng, 8)
-    r3 = rng.uniform(0.7 ** 3, 1.0 ** 3, 8)
-    centres = dirs * np.cbrt(r3)[:, None]
+    d = unit_vectors(rng, 1)[0]
+
+    def around(m, lo, hi):
+        """m unit vectors at angular distance U[lo, hi] from d, uniform azimuth."""
+        a = np.cross(d, [0.0, 0.0, 1.0] if abs(d[2]) < 0.9 else [1.0, 0.0, 0.0])
+        a /= np.linalg.norm(a)
+        b = np.cross(d, a)
+        ang = rng.uniform(lo, hi, m)
+        az = rng.uniform(0.0, 2 * np.pi, m)
+        return (np.cos(ang)[:, None] * d + np.sin(ang)[:, None] *
+                (np.cos(az)[:, None] * a + np.sin(az)[:, None] * b))
+
+    centres = around(8, 0.03, 0.2) * rng.uniform(0.9, 0.97, (8, 1))
     blobs = [(tuple(centres[i]), 0.03, 0.01) for i in range(8)]
-    rec = unit_vectors(rng, 32) * receiver_r
-    d = unit_vectors(rng, 1)[0] * 0.95
+    rec = around(32, 0.05, 0.25) * receiver_r
     return Config("c4", nx, nr, model, cfl_dt(nx, model), nsteps, outer_sponge(nr),
-                  [Source(tuple(d), 0.02, 1.0)], dc_blobs=blobs, receivers=rec)
+                  [Source(tuple(d * 0.95), 0.02, 1.0)], dc_blobs=blobs, receivers=rec)
 
 
 def c5(nx: int = 384, nsteps: int = 200, nsrc: int = 16) -> Config:

@@ -645,7 +645,16 @@ int solar_gpu_rk4(solar_ctx* c, int nsteps) {
   return check_device_error(c);
 }
 
-int solar_gpu_rk4_runs(solar_ctx* c, const int* nsteps_per_run) {
+static int rk4_runs_impl(solar_ctx* c, const int* nsteps_per_run, double* ms);
+
+int solar_gpu_rk4_runs(solar_ctx* c, const int* nsteps_per_run) { return rk4_runs_impl(c, nsteps_per_run, nullptr); }
+
+int solar_gpu_time_rk4_runs(solar_ctx* c, const int* nsteps_per_run, double* ms) {
+  if (!ms) return fail(SOLAR_ERR_ARG, "null output");
+  return rk4_runs_impl(c, nsteps_per_run, ms);
+}
+
+static int rk4_runs_impl(solar_ctx* c, const int* nsteps_per_run, double* ms) {
   int rc = check_ctx(c);
   if (rc) return rc;
   if (!nsteps_per_run) return fail(SOLAR_ERR_ARG, "null step counts");
@@ -658,8 +667,15 @@ int solar_gpu_rk4_runs(solar_ctx* c, const int* nsteps_per_run) {
   CK(cudaMemcpyAsync(c->target, nsteps_per_run, R * sizeof(int), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemsetAsync(c->done, 0, R * sizeof(int), c->stream));
   if ((rc = capture_batch_graph(c))) return rc;
+  CK(cudaEventRecord(c->ev[0], c->stream));
   for (int s = 0; s < maxs; ++s) CK(cudaGraphLaunch(c->batch_graph, c->stream));
+  CK(cudaEventRecord(c->ev[1], c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  if (ms) {
+    float f = 0.f;
+    CK(cudaEventElapsedTime(&f, c->ev[0], c->ev[1]));
+    *ms = f;
+  }
   return check_device_error(c);
 }
 

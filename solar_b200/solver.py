@@ -137,6 +137,16 @@ class Solver:
             raise ValueError("need one step count per run")
         _lib.check(self.lib.solar_gpu_rk4_runs(self._h, s.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
 
+    def time_rk4_runs(self, steps: Sequence[int]) -> float:
+        """rk4_runs, returning the batch's device time in ms (CUDA events)."""
+        s = np.ascontiguousarray(np.asarray(steps, dtype=np.int32))
+        if s.shape != (self.nruns,):
+            raise ValueError("need one step count per run")
+        ms = ctypes.c_double()
+        _lib.check(self.lib.solar_gpu_time_rk4_runs(self._h, s.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                                    ctypes.byref(ms)))
+        return ms.value
+
     # ------------------------------------------------------------------ operators
     def compute_rhs(self, q: np.ndarray) -> np.ndarray:
         q = np.ascontiguousarray(q, dtype=np.float64)
