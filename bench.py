@@ -307,6 +307,39 @@ def large_block(device: int, nsteps: int):
     return out
 
 
+def split_block(cfg, args, world, local):
+    """Zones split across the job's processes (strong scaling of one six-zone run): each
+    rank owns 6/world zones and exchanges edge lines with its neighbours every phase over
+    torch.distributed (NCCL).  Timed with CUDA events on the library's stream, max over
+    ranks."""
+    import torch
+
+    import torch.distributed as dist
+
+    from solar_b200 import distributed as D
+
+    if not dist.is_initialized():             # one process: a one-rank group
+        import socket
+        with socket.socket() as sk:
+            sk.bind(("127.0.0.1", 0))
+            port = sk.getsockname()[1]
+        dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1)
+    zs = D.ZoneSplitSolver(cfg, precision="fp32", nfields=4, device=local)
+    zs.solver.init_sources()
+    zs.rk4(args.warmup)
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(zs.stream)
+    zs.rk4(args.steps)
+    e1.record(zs.stream)
+    e1.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    norm = zs.norm(4)
+    zs.close()
+    return {"value": cfg.points * args.steps / (ms / 1e3), "unit": "grid-pt RK4 updates/s", "scaling": "strong",
+            "ms_per_step": ms / args.steps, "zones_per_rank": 6 // world, "norm_vr": norm}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -320,6 +353,8 @@ def main():
     ap.add_argument("--adjoint-steps", type=int, default=500)
     ap.add_argument("--adjoint-checkpoint", type=int, default=50)
     ap.add_argument("--adjoint-fd", type=int, default=4)
+    ap.add_argument("--split", action="store_true",
+                    help="also run the zones split across the job's processes (world must divide 6)")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-large", action="store_true")
     ap.add_argument("--large-steps", type=int, default=200)
@@ -403,6 +438,7 @@ def main():
                "note": "state in from pinned host memory once, RK4 + norm(v_r) read back every step "
                        "(cube.f90:74-78), state out at the end; timed per job of K steps"}
 
+    split = split_block(cfg, args, world, local) if args.split else None
     if rank != 0:
         return
     adjoint = batch = large = None
@@ -445,6 +481,7 @@ def main():
         "adjoint": adjoint,
         "batched_sources": batch,
         "large_grid": large,
+        "zone_split": split,
     }
     print(json.dumps(line), flush=True)
 

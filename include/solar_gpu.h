@@ -156,6 +156,46 @@ int solar_gpu_time_rk4(solar_ctx* c, int nsteps, int per_kernel, double* out7);
 /* Block until the context's stream is idle. */
 int solar_gpu_synchronize(solar_ctx* c);
 
+/* ---- Zones split across processes (one GPU per process, nruns == 1) ---------------
+ * The reference runs one MPI rank per zone block and exchanges interpolated halo strips
+ * inside every derivative (derivative.f90:8-323).  Here a context can own a contiguous
+ * range of zones: the step kernels then run on those zones only.  Every ghost value of an
+ * owned zone is interpolated from the three lines next to one edge of a neighbouring zone
+ * (the route table); where that zone belongs to another process, the host moves those
+ * lines between the phases of a step: pack on the owner, transfer (e.g. NCCL send/recv on
+ * the context's stream), unpack on the receiver, then run the phase.
+ *
+ * Owned zones zone0 .. zone0+nzones-1 (0-based); the default is all six.  Diagnostics
+ * (solar_gpu_norm, solar_gpu_diag) then cover the owned zones only. */
+int solar_gpu_set_owned_zones(solar_ctx* c, int zone0, int nzones);
+
+/* routes[(z*4+e)*3 + {0,1,2}] = (source zone, source edge, reversed) of the ghost frame of
+ * zone z (0-based) at edge e (0 S, 1 N, 2 W, 3 E): derivative.f90's halo routing. */
+int solar_gpu_edge_routes(int* routes);
+
+/* One phase of an RK4 call, enqueued on the context's stream (no wait): phases 0..4 are
+ * the five stages (edge exchange of p, v_xi, v_eta + fused stage kernel), phase 5 is
+ * FILTER_EXP (edge exchange of every field + filter).  Phases 0..5 in order = one
+ * solar_gpu_rk4(c, 1). */
+int solar_gpu_step_phase(solar_ctx* c, int phase);
+
+/* Values (of the context's precision) in the packed lines of one (zone, edge) pair in
+ * phase `phase`: 3 * nx * nr * (3 fields in phases 0..4, every stored field in phase 5). */
+long long solar_gpu_lines_size(solar_ctx* c, int phase);
+
+/* Copy the source lines of `count` (zone, edge) pairs (zone_edge[2q], zone_edge[2q+1]) of
+ * the buffer that phase `phase` reads into / out of the device buffer d_buf
+ * (count * solar_gpu_lines_size values).  Enqueued on the context's stream. */
+int solar_gpu_pack_lines(solar_ctx* c, int phase, const int* zone_edge, int count, void* d_buf);
+int solar_gpu_unpack_lines(solar_ctx* c, int phase, const int* zone_edge, int count, const void* d_buf);
+
+/* The context's CUDA stream (a cudaStream_t), to order the caller's transfers with it. */
+void* solar_gpu_stream(solar_ctx* c);
+
+/* Raw partial sums over the owned zones of run `run`, for a cross-process reduction:
+ * out5 = (sum of field^2 (field 1..5; 0 = none), energy, mass, max |p|, non-finite count). */
+int solar_gpu_reduce_owned(solar_ctx* c, int run, int field, double* out5);
+
 /* ---- Discrete adjoint (run 0 of a context with nruns == 1) -------------------------
  * No counterpart in the reference, which has no adjoint.  These are the exact transposes
  * of the discrete forward operators above: COMPUTE_RHS + BC_RHS + SPONGE, FILTER_EXP

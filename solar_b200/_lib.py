@@ -76,7 +76,19 @@ EXPORTS = {
     "solar_gpu_rhs_adjoint": [_P, _D, _D],
     "solar_gpu_filter_adjoint": [_P, _D, _D],
     "solar_gpu_rk4_adjoint": [_P, ctypes.c_int, _D, _D],
+    "solar_gpu_set_owned_zones": [_P, ctypes.c_int, ctypes.c_int],
+    "solar_gpu_edge_routes": [_I],
+    "solar_gpu_step_phase": [_P, ctypes.c_int],
+    "solar_gpu_lines_size": [_P, ctypes.c_int],
+    "solar_gpu_pack_lines": [_P, ctypes.c_int, _I, ctypes.c_int, ctypes.c_void_p],
+    "solar_gpu_unpack_lines": [_P, ctypes.c_int, _I, ctypes.c_int, ctypes.c_void_p],
+    "solar_gpu_stream": [_P],
+    "solar_gpu_reduce_owned": [_P, ctypes.c_int, ctypes.c_int, _D],
 }
+
+# entry points whose return type is not int
+RESTYPES = {"solar_desc_defaults": None, "solar_gpu_lines_size": ctypes.c_longlong,
+            "solar_gpu_stream": ctypes.c_void_p}
 
 _lib = None
 
@@ -100,7 +112,7 @@ def load(build_if_missing: bool = False):
     for name, args in EXPORTS.items():
         fn = getattr(lib, name)
         fn.argtypes = args
-        fn.restype = None if name == "solar_desc_defaults" else ctypes.c_int
+        fn.restype = RESTYPES.get(name, ctypes.c_int)
     _lib = lib
     return lib
 

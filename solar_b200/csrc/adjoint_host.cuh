@@ -12,6 +12,7 @@ static long long state_bytes(const solar_ctx* c) { return 6LL * c->g.nf * c->g.v
 
 static int adj_alloc(solar_ctx* c) {
   AdjBuffers& b = c->adj;
+  if (c->g.nface != 6) return fail(SOLAR_ERR_ARG, "the adjoint entry points need a context owning all six zones");
   if (b.L) return SOLAR_OK;
   if (c->g.nruns != 1) return fail(SOLAR_ERR_ARG, "the adjoint entry points need nruns == 1");
   const size_t S = (size_t)state_bytes(c);

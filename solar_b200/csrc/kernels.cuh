@@ -35,6 +35,7 @@ struct Geom {
   long long plane, vs;      // padded plane size; volume stride (per run/face/field)
   int nruns;
   int slot[5];              // slot of each reference field, -1 if not stored
+  int face0, nface;         // zones the step kernels work on (a process owning part of the sphere)
   __host__ __device__ long long vol(int run, int face, int s) const {
     return ((long long)(run * 6 + face) * nf + s) * vs;
   }
@@ -137,7 +138,7 @@ __global__ void __launch_bounds__(128) edge_kernel(const EdgeArgs<T> a) {
   T* buf = reinterpret_cast<T*>(esm);                    // [field][kk][layer][t_s]
   const Geom& g = a.g;
   const int n = g.n;
-  const int fe = blockIdx.y, face = fe >> 2, e = fe & 3, run = blockIdx.z;
+  const int fe = g.face0 * 4 + blockIdx.y, face = fe >> 2, e = fe & 3, run = blockIdx.z;
   if (a.active && !a.active[run]) return;
   const int kb = blockIdx.x * KC;
   if (kb >= g.nr) return;
@@ -340,7 +341,7 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __
   const int n = g.n, nr = g.nr;
   const int tiles_x = n / TX;
   const int i0 = (blockIdx.x % tiles_x) * TX, j0 = (blockIdx.x / tiles_x) * TY;
-  const int rf = blockIdx.z, run = rf / 6, face = rf % 6;
+  const int run = blockIdx.z / g.nface, face = g.face0 + blockIdx.z % g.nface;
   if (a.active && !a.active[run]) return;
   const int kb = blockIdx.y * a.kchunk;
   if (kb >= nr) return;
@@ -641,7 +642,7 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) filter_kernel(const _
   const int tiles_x = n / TX;
   const int i0 = (blockIdx.x % tiles_x) * TX, j0 = (blockIdx.x / tiles_x) * TY;
   const int s = blockIdx.y;                  // stored field
-  const int rf = blockIdx.z, run = rf / 6, face = rf % 6;
+  const int run = blockIdx.z / g.nface, face = g.face0 + blockIdx.z % g.nface;
   if (a.active && !a.active[run]) return;
   const int cx = threadIdx.x, ty = threadIdx.y, tid = ty * NT + cx;
   constexpr int PW = TX + 8;
@@ -754,6 +755,38 @@ __global__ void strip_extract_kernel(const T* __restrict__ q, T* __restrict__ st
   strips[idx] = q[g.vol(run, face, s) + g.at(k, jj, ii)];
 }
 
+// Edge lines exchanged between processes that own different zones: for item q the
+// (zone, edge) pair items[2q], items[2q+1]; the three lines next to that edge that the
+// neighbouring zone interpolates from (rows 1..3 / n-2..n-4, columns likewise), for the
+// slots listed in `slots`.  Packed layout [item][slot][k][layer][t], t along the edge.
+template <typename T>
+__device__ __forceinline__ long long line_offset(const Geom& g, int face, int e, int s, int k, int l, int t) {
+  const int n = g.n;
+  int ii, jj;
+  if (e == 0) { ii = t; jj = l + 1; }
+  else if (e == 1) { ii = t; jj = n - 2 - l; }
+  else if (e == 2) { ii = l + 1; jj = t; }
+  else { ii = n - 2 - l; jj = t; }
+  return g.vol(0, face, s) + g.at(k, jj, ii);
+}
+
+template <typename T>
+__global__ void line_pack_kernel(const T* __restrict__ q, T* __restrict__ out, const int* __restrict__ items,
+                                 int nitems, const int* __restrict__ slots, int nslots, Geom g, int unpack) {
+  const long long per = (long long)3 * g.n * g.nr;          // one slot of one item
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= per * nslots * nitems) return;
+  const int t = idx % g.n;
+  long long r = idx / g.n;
+  const int l = r % 3; r /= 3;
+  const int k = r % g.nr; r /= g.nr;
+  const int si = r % nslots;
+  const int it = (int)(r / nslots);
+  const long long o = line_offset<T>(g, items[2 * it], items[2 * it + 1], slots[si], k, l, t);
+  if (unpack) const_cast<T*>(q)[o] = out[idx];
+  else out[idx] = q[o];
+}
+
 // ---------------------------------------------------------------------------------
 // State transfer: six-zone Fortran-order FP64 arrays <-> padded device volumes.
 // One launch moves one (face, reference field) volume.
@@ -827,7 +860,7 @@ template <typename T>
 __global__ void reduce_plane_kernel(const T* q, Geom g, int run, int sel_slot, const double* rad64,
                                     const double* vol2, const double* drw, const double* c2_3d,
                                     double* part) {
-  const int face = blockIdx.x / g.nr, k = blockIdx.x % g.nr;
+  const int face = g.face0 + blockIdx.x / g.nr, k = blockIdx.x % g.nr;
   const int n = g.n;
   double acc[5] = {0, 0, 0, 0, 0};
   const double rho0 = rad64[rRho0 * g.nr + k];

@@ -103,6 +103,8 @@ struct solar_ctx {
   cudaGraphExec_t batch_graph = nullptr;
   cudaEvent_t ev[8] = {};
   AdjBuffers adj;
+  int* split_items = nullptr;  // (zone, edge) pairs of one line pack/unpack
+  int* split_slots = nullptr;  // slots exchanged per phase
 };
 
 namespace solar {
@@ -200,7 +202,7 @@ static int launch_edge(solar_ctx* c, void* buf, int mode, const int* active) {
       attr_set = true;
     }
   }
-  dim3 grid((c->g.nr + kEdgePlanes - 1) / kEdgePlanes, 24, c->g.nruns);
+  dim3 grid((c->g.nr + kEdgePlanes - 1) / kEdgePlanes, 4 * c->g.nface, c->g.nruns);
   edge_kernel<T, kEdgePlanes><<<grid, 128, smem, c->stream>>>(a);
   return SOLAR_OK;
 }
@@ -219,7 +221,7 @@ static int launch_stage_t(solar_ctx* c, StageArgs<T>& a, const void* qin) {
     attr_set = true;
   }
   const int nchunks = (c->g.nr + a.kchunk - 1) / a.kchunk;
-  dim3 grid((c->g.n / TX) * (c->g.n / TY), nchunks, c->g.nruns * 6);
+  dim3 grid((c->g.n / TX) * (c->g.n / TY), nchunks, c->g.nruns * c->g.nface);
   stage_kernel<T, TX, TY, MODE, HAS_RHO><<<grid, dim3(TX / Vec16<T>::V, TY), L::TOTAL, c->stream>>>(a);
   return SOLAR_OK;
 }
@@ -283,7 +285,7 @@ static int launch_filter_t(solar_ctx* c, const void* qin, void* qout, const int*
     CK(cudaFuncSetAttribute(filter_kernel<T, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::TOTAL));
     attr_set = true;
   }
-  dim3 grid((c->g.n / TX) * (c->g.n / TY), c->g.nf, c->g.nruns * 6);
+  dim3 grid((c->g.n / TX) * (c->g.n / TY), c->g.nf, c->g.nruns * c->g.nface);
   filter_kernel<T, TX, TY><<<grid, dim3(TX / Vec16<T>::V, TY), L::TOTAL, c->stream>>>(a);
   return SOLAR_OK;
 }
@@ -428,7 +430,7 @@ static int check_ctx(solar_ctx* c) {
 }
 
 static int reduce(solar_ctx* c, int run, int sel_field, double* out5) {
-  const int nblocks = 6 * c->g.nr;
+  const int nblocks = c->g.nface * c->g.nr;
   const int sel = (sel_field >= 0 && sel_field < 5) ? c->g.slot[sel_field] : -1;
   if (c->fp32)
     reduce_plane_kernel<float><<<nblocks, 256, 0, c->stream>>>((const float*)c->A, c->g, run, sel, c->dt.rad64,
@@ -491,7 +493,7 @@ int solar_gpu_finalize(solar_ctx* c) {
   for (void* p : ptrs)
     if (p) cudaFree(p);
   void* aptrs[] = {c->adj.L, c->adj.LW, c->adj.T1, c->adj.T2, c->adj.I, c->adj.grad, c->adj.ckpt,
-                   c->adj.div, c->adj.traces, c->adj.rec_off, c->adj.rec_w};
+                   c->adj.div, c->adj.traces, c->adj.rec_off, c->adj.rec_w, c->split_items, c->split_slots};
   for (void* p : aptrs)
     if (p) cudaFree(p);
   for (auto& e : c->ev)
@@ -530,6 +532,8 @@ int solar_gpu_init(const solar_desc* d, solar_ctx** out) {
   g.plane = (long long)g.pitch * g.rows;
   g.vs = g.plane * g.nr;   // volumes back to back: the whole buffer is one 3-D array of planes
   g.nruns = d->nruns;
+  g.face0 = 0;
+  g.nface = 6;
   if (g.nf == 5) { for (int f = 0; f < 5; ++f) g.slot[f] = f; }
   else { g.slot[kRho] = -1; g.slot[kVxi] = 0; g.slot[kVeta] = 1; g.slot[kVr] = 2; g.slot[kP] = 3; }
   // tile choice (16x16, 32x8, 32x16, 64x8)
@@ -849,9 +853,11 @@ int solar_gpu_synchronize(solar_ctx* c) {
   int rc = check_ctx(c);
   if (rc) return rc;
   CK(cudaStreamSynchronize(c->stream));
-  return SOLAR_OK;
+  CK(cudaGetLastError());
+  return check_device_error(c);
 }
 
 }  // extern "C"
 
 #include "adjoint_host.cuh"
+#include "split_host.cuh"

@@ -1,0 +1,222 @@
+"""Zones split across processes, one GPU per process.
+
+The reference decomposes the sphere into zone blocks, one MPI rank each (init_mpi.f90),
+and exchanges interpolated 3-deep halo strips inside every derivative and filter
+(derivative.f90:8-323, filter.f90:9-48, routed by the intercommunicator partner map of
+init_mpi.f90:164-304).  Here each process owns a contiguous range of the six zones and
+runs the same fused kernels on them (``solar_gpu_set_owned_zones``).  Before each phase of
+a step (five stages, then the filter) it sends, to every process owning a neighbouring
+zone, the three raw lines next to each shared edge; the receiver interpolates and rotates
+them into its ghost frame with its own edge kernel, exactly as for a zone it owns.  One
+message per peer and phase: 3 * nx * nr values per (zone, edge) pair and exchanged field.
+
+The plan (which pairs go where, in which order) is pure host logic and is tested on CPU
+with the gloo backend; the transfer is ``torch.distributed`` point-to-point (NCCL between
+GPUs) ordered on the library's CUDA stream.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Dict, List, Sequence, Tuple
+
+import numpy as np
+
+from . import _lib
+
+Pair = Tuple[int, int]            # (source zone, source edge), 0-based; edges 0 S, 1 N, 2 W, 3 E
+
+
+def partition(world: int) -> List[Tuple[int, int]]:
+    """Contiguous zone ranges (zone0, nzones) of each rank; world must divide 6."""
+    if world < 1 or 6 % world:
+        raise ValueError(f"zone splitting needs 1, 2, 3 or 6 processes, not {world}")
+    per = 6 // world
+    return [(r * per, per) for r in range(world)]
+
+
+def route_table() -> np.ndarray:
+    """(6, 4, 3) array: for receiving zone z and edge e, (source zone, source edge,
+    reversed) -- the library's copy of the reference's halo routing."""
+    out = (ctypes.c_int * 72)()
+    _lib.check(_lib.load().solar_gpu_edge_routes(out))
+    return np.array(out, dtype=np.int64).reshape(6, 4, 3)
+
+
+def owners(parts: Sequence[Tuple[int, int]]) -> List[int]:
+    own = [-1] * 6
+    for r, (z0, nz) in enumerate(parts):
+        for z in range(z0, z0 + nz):
+            own[z] = r
+    return own
+
+
+def exchange_plan(routes: np.ndarray, parts: Sequence[Tuple[int, int]], rank: int):
+    """(sends, recvs): for each peer rank, the ordered (zone, edge) source pairs this rank
+    sends to / receives from it.  Both sides enumerate receivers in the same global order
+    (receiving zone, then edge), so the lists of a sender and its receiver match."""
+    own = owners(parts)
+    sends: Dict[int, List[Pair]] = {}
+    recvs: Dict[int, List[Pair]] = {}
+    for z in range(6):
+        for e in range(4):
+            sz, se = int(routes[z, e, 0]), int(routes[z, e, 1])
+            src, dst = own[sz], own[z]
+            if src == dst:
+                continue
+            if src == rank:
+                sends.setdefault(dst, []).append((sz, se))
+            if dst == rank:
+                recvs.setdefault(src, []).append((sz, se))
+    return sends, recvs
+
+
+def _pairs_array(pairs: Sequence[Pair]):
+    a = (ctypes.c_int * (2 * len(pairs)))()
+    for q, (z, e) in enumerate(pairs):
+        a[2 * q], a[2 * q + 1] = z, e
+    return a
+
+
+class LineExchange:
+    """Moves the edge lines of one phase between ranks.
+
+    ``packer`` provides ``size(phase)`` (values per pair), ``pack(phase, pairs, buf)`` and
+    ``unpack(phase, pairs, buf)``; ``transport(sends, recvs)`` delivers every send buffer to
+    its peer and fills every receive buffer (``{peer: buffer}`` dicts).  ``alloc(n)``
+    returns an n-value buffer."""
+
+    def __init__(self, plan, packer, transport, alloc):
+        self.sends, self.recvs = plan
+        self.packer, self.transport = packer, transport
+        self._buf = {}
+        for kind, phase in (("stage", 0), ("filter", 5)):
+            per = packer.size(phase)
+            self._buf[kind] = ({p: alloc(len(v) * per) for p, v in self.sends.items()},
+                               {p: alloc(len(v) * per) for p, v in self.recvs.items()})
+
+    @property
+    def empty(self) -> bool:
+        return not self.sends and not self.recvs
+
+    def buffers(self, phase: int):
+        """({peer: send buffer}, {peer: receive buffer}) of this phase."""
+        return self._buf["filter" if phase == 5 else "stage"]
+
+    def pack(self, phase: int) -> None:
+        sbuf, _ = self.buffers(phase)
+        for peer, pairs in self.sends.items():
+            self.packer.pack(phase, pairs, sbuf[peer])
+
+    def unpack(self, phase: int) -> None:
+        _, rbuf = self.buffers(phase)
+        for peer, pairs in self.recvs.items():
+            self.packer.unpack(phase, pairs, rbuf[peer])
+
+    def run(self, phase: int) -> None:
+        if self.empty:
+            return
+        self.pack(phase)
+        self.transport(*self.buffers(phase))
+        self.unpack(phase)
+
+
+class _LibPacker:
+    """pack/unpack through the C-ABI into CUDA tensors, on the context's stream."""
+
+    def __init__(self, solver):
+        self.s = solver
+
+    def size(self, phase):
+        return int(self.s.lib.solar_gpu_lines_size(self.s._h, phase))
+
+    def pack(self, phase, pairs, buf):
+        _lib.check(self.s.lib.solar_gpu_pack_lines(self.s._h, phase, _pairs_array(pairs), len(pairs),
+                                                   ctypes.c_void_p(buf.data_ptr())))
+
+    def unpack(self, phase, pairs, buf):
+        _lib.check(self.s.lib.solar_gpu_unpack_lines(self.s._h, phase, _pairs_array(pairs), len(pairs),
+                                                     ctypes.c_void_p(buf.data_ptr())))
+
+
+def p2p_transport(stream=None, group=None):
+    """torch.distributed point-to-point exchange, issued on ``stream`` (a torch stream;
+    the library's stream for GPU buffers) so that it is ordered after the packing and
+    before the unpacking."""
+    import contextlib
+
+    import torch
+    import torch.distributed as dist
+
+    def run(sends, recvs):
+        ctx = torch.cuda.stream(stream) if stream is not None else contextlib.nullcontext()
+        with ctx:
+            ops = [dist.P2POp(dist.isend, b, p, group) for p, b in sorted(sends.items())]
+            ops += [dist.P2POp(dist.irecv, b, p, group) for p, b in sorted(recvs.items())]
+            for req in dist.batch_isend_irecv(ops):
+                req.wait()
+    return run
+
+
+class ZoneSplitSolver:
+    """One rank's share of a six-zone run: owns ``partition(world)[rank]`` zones of a
+    :class:`solar_b200.solver.Solver` on this process's GPU and exchanges edge lines with
+    the other ranks every phase.  ``torch.distributed`` must be initialised (NCCL)."""
+
+    def __init__(self, cfg, precision: str = "fp64", nfields: int = 5, device: int = 0, group=None, **kw):
+        import torch
+        import torch.distributed as dist
+
+        from .solver import Solver
+
+        self.world = dist.get_world_size(group)
+        self.rank = dist.get_rank(group)
+        self.group = group
+        self.parts = partition(self.world)
+        self.zone0, self.nzones = self.parts[self.rank]
+        self.solver = Solver(cfg, precision=precision, nfields=nfields, device=device, **kw)
+        s = self.solver
+        _lib.check(s.lib.solar_gpu_set_owned_zones(s._h, self.zone0, self.nzones))
+        self.stream = torch.cuda.ExternalStream(s.lib.solar_gpu_stream(s._h), device=torch.device("cuda", device))
+        dtype = torch.float32 if precision == "fp32" else torch.float64
+        plan = exchange_plan(route_table(), self.parts, self.rank)
+        self.exchange = LineExchange(plan, _LibPacker(s), p2p_transport(self.stream, group),
+                                     lambda n: torch.empty(n, dtype=dtype, device=torch.device("cuda", device)))
+
+    def set_state(self, q: np.ndarray) -> None:
+        """Every rank loads the whole six-zone state (it computes only its own zones)."""
+        self.solver.set_state(q)
+
+    def rk4(self, nsteps: int = 1) -> None:
+        s = self.solver
+        for _ in range(int(nsteps)):
+            for phase in range(6):
+                self.exchange.run(phase)
+                _lib.check(s.lib.solar_gpu_step_phase(s._h, phase))
+        s.synchronize()
+
+    def norm(self, field: int = 4) -> float:
+        """auxiliary.f90:100-125 over the whole sphere: owned partial sums, all-reduced."""
+        import torch
+        import torch.distributed as dist
+
+        out = (ctypes.c_double * 5)()
+        _lib.check(self.solver.lib.solar_gpu_reduce_owned(self.solver._h, 0, field, out))
+        t = torch.tensor([out[0]], dtype=torch.float64, device=torch.device("cuda", torch.cuda.current_device()))
+        dist.all_reduce(t, group=self.group)
+        n, nr = self.solver.nx, self.solver.nr
+        return float((t.item() / (n * n * nr) * 6.0) ** 0.5)
+
+    def gather_state(self) -> np.ndarray:
+        """The whole six-zone state, assembled from every rank's owned zones."""
+        import torch.distributed as dist
+
+        q = self.solver.get_state()
+        mine = (self.zone0, q[self.zone0:self.zone0 + self.nzones])
+        allp = [None] * self.world
+        dist.all_gather_object(allp, mine, group=self.group)
+        for z0, part in allp:
+            q[z0:z0 + len(part)] = part
+        return q
+
+    def close(self) -> None:
+        self.solver.close()
