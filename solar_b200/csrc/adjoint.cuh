@@ -9,12 +9,12 @@
 // (c -> c + dc enters only r_p = -c^2 rho0 div v, compute_rhs_acoustic.f90:134) gathers
 //     g += dt (-2 c rho0 div(v_{s-1})) mu_s^p            (0 on the BC planes).
 // L^T is applied in three kernels:
-//   adj_pre    pointwise: mu, the BC mask, the coefficient-weighted fields whose transposed
-//              derivatives make up L^T, the pointwise terms, the sponge, lw and g;
-//   adj_deriv  transposed derivatives: -D_xi and -D_eta with zero halos (the DRP stencil is
-//              antisymmetric), the radial transpose written out row by row (one-sided rows
-//              and the dr/dchi metric), evaluated on the interior and on the ghost frame --
-//              the frame values are the adjoints of the neighbour faces' ghost values;
+//   adj_stage  mu, the BC mask, the pointwise terms, the sponge, lw and g, and the
+//              transposed derivatives of the coefficient-weighted fields: -D_xi and -D_eta
+//              with zero halos (the DRP stencil is antisymmetric) and the banded radial
+//              transpose, on the interior and on the ghost frame -- the frame values are the
+//              adjoints of the neighbour faces' ghost values;
+//   adj_rbdy   the one-sided (Tam-Dong) rows of the radial transpose;
 //   adj_edge   the transpose of the edge exchange: ghost adjoints scattered (atomic adds)
 //              into the source faces' lines with the same folded coefficients.
 // FILTER_EXP^T is the radial transpose, then eta, then xi, each with its ghost-frame
@@ -25,183 +25,274 @@
 
 namespace solar {
 
+// Fused transposed stage: adj_pre_kernel + adj_deriv_kernel in one pass over the state.
+// A CTA owns a TX x TY column tile of one face and marches the planes of its chunk (plus
+// three planes on either side for the radial window).  Per plane it forms the
+// coefficient-weighted volumes X1, X2 (on the tile and its xi halo) and Y1, Y2 (tile and
+// eta halo) in shared memory from mu = lw + beta lq of that plane (zero outside the face
+// and on the BC planes), applies -D_xi / -D_eta, and keeps facr * R1 and facr * R2 of the
+// last seven planes in registers for the banded part of the radial transpose, which
+// completes plane k three iterations later.  The rows of the one-sided radial stencil
+// (planes 1, 2, nr-3, nr-2; planes 0 and nr-1 carry zero) are written to `rb` and
+// added by adj_rbdy_kernel.  Edge tiles also write the ghost-frame adjoints.  Inputs
+// (lq, lw) and outputs (lout, lwout) are distinct buffers: neighbouring CTAs read the
+// inputs' halos.
 template <typename T>
-struct AdjArgs {
-  const T* lq;        // lambda_q of the stage output (padded, interior)
-  T* lw;              // lambda_w, updated in place
-  T* lout;            // lambda_q of the stage input: interior + ghost-frame adjoints
-  T* inter;           // 6 intermediate volumes per (run, face): X1 Y1 R1 X2 Y2 R2, zero frames
-  const T* div;       // compact [run][face][k][j][i] divergence of the stage input (BC-masked)
-  const T* c2;        // optional per-point c^2 [face][k][j][i] or nullptr (radial)
-  double* grad;       // compact [run][face][k][j][i] gradient accumulator, or nullptr
+struct AdjStageArgs {
+  const T* lq;
+  const T* lw;
+  T* lout;
+  T* lwout;
+  T* rb;              // [face][4][2][n*n] raw R1, R2 of planes 1, 2, nr-3, nr-2
+  const T* div;       // compact stage-input divergence, or nullptr
+  const T* c2;
+  double* grad;
   const T* rad;
   const T* met;
   Geom g;
   T alpha, beta, dt, inv_dxi;
-  int keep;           // 1: lout = lq + dt L^T mu (RK adjoint); 0: lout = L^T mu (operator)
+  int keep, kchunk;
 };
 
-__device__ __forceinline__ long long inter_vol(const Geom& g, int run, int face, int m) {
-  return ((long long)(run * 6 + face) * 6 + m) * g.vs;
-}
-
-template <typename T>
-__global__ void adj_pre_kernel(const AdjArgs<T> a) {
+template <typename T, int TX, int TY>
+__global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const AdjStageArgs<T> a) {
+  constexpr int XW = TX + 6, YH = TY + 6;
+  constexpr int NHALO = 6 * TX + 6 * TY;
+  static_assert(NHALO <= TX * TY, "one halo point per thread");
+  __shared__ T sX1[TY][XW], sX2[TY][XW], sY1[YH][TX], sY2[YH][TX];
   const Geom& g = a.g;
   const int n = g.n, nr = g.nr;
-  const long long V = (long long)n * n * nr;
-  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= (long long)g.nruns * 6 * V) return;
-  const int rf = idx / V, run = rf / 6, face = rf % 6;
-  const long long l = idx % V;
-  const int i = l % n, j = (l / n) % n, k = l / ((long long)n * n);
-  const long long pt = g.at(k, j, i);
   const long long P2 = (long long)n * n;
+  const int tiles_x = n / TX;
+  const int i0 = (blockIdx.x % tiles_x) * TX, j0 = (blockIdx.x / tiles_x) * TY;
+  const int face = blockIdx.z;
+  const int kb = blockIdx.y * a.kchunk, ke = min(nr, kb + a.kchunk);
+  if (kb >= nr) return;
+  const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
+  const int i = i0 + tx, j = j0 + ty;
   const int p2 = j * n + i;
-  T mu[5], muq[5];
-#pragma unroll
-  for (int f = 0; f < 5; ++f) {
-    const int s = g.slot[f];
-    if (s < 0) { mu[f] = muq[f] = T(0); continue; }
-    const long long o = g.vol(run, face, s) + pt;
-    const T lq = a.lq[o];
-    muq[f] = lq;
-    mu[f] = a.lw[o] + a.beta * lq;
-    a.lw[o] = a.alpha * mu[f];
+  const int sRho = g.slot[kRho], sX = g.slot[kVxi], sY = g.slot[kVeta], sR = g.slot[kVr], sP = g.slot[kP];
+  const T* __restrict__ lq = a.lq;
+  const T* __restrict__ lw = a.lw;
+  const T* __restrict__ met = a.met;
+  const T* __restrict__ rad = a.rad;
+  const T tD = __ldg(met + mD * P2 + p2), tXYD = __ldg(met + mXYD * P2 + p2), tC = __ldg(met + mC * P2 + p2);
+  const T tXYC = __ldg(met + mXYC * P2 + p2), tDivX = __ldg(met + mDivX * P2 + p2), tDivY = __ldg(met + mDivY * P2 + p2);
+  const T tTX = __ldg(met + mTX * P2 + p2), tTY = __ldg(met + mTY * P2 + p2);
+  const T c1 = Coef<T>::drp(1), c2c = Coef<T>::drp(2), c3 = Coef<T>::drp(3);
+  // this thread's halo point: eta-halo rows first, then xi-halo columns
+  bool has_halo = tid < NHALO, xi_halo = false;
+  int hi = 0, hj = 0;
+  if (tid < 6 * TX) { hi = tid % TX; const int r = tid / TX; hj = r < 3 ? r - 3 : TY + r - 3; }
+  else if (has_halo) { xi_halo = true; const int q = tid - 6 * TX; hj = q % TY; const int cc = q / TY; hi = cc < 3 ? cc - 3 : TX + cc - 3; }
+  const int hgi = i0 + hi, hgj = j0 + hj;
+  const bool h_in = has_halo && hgi >= 0 && hgi < n && hgj >= 0 && hgj < n;
+  const int hq2 = h_in ? hgj * n + hgi : 0;
+  T hm1 = T(0), hm2 = T(0);       // halo point metric: (D, XY/C, DivX) for xi, (XY/D, C, DivY) for eta
+  T hm3 = T(0);
+  if (h_in) {
+    hm1 = __ldg(met + (xi_halo ? mD : mXYD) * P2 + hq2);
+    hm2 = __ldg(met + (xi_halo ? mXYC : mC) * P2 + hq2);
+    hm3 = __ldg(met + (xi_halo ? mDivX : mDivY) * P2 + hq2);
   }
-  const bool bc = (k == 0 || k == nr - 1);
-  T mp[5];
+  auto vol = [&](int s) { return g.vol(0, face, s); };
+  T w1[7], w2[7];          // facr * R1, facr * R2 of planes m-6 .. m (banded rows only)
+  T pp[4], pv[4];          // partial outputs of p and v_r, planes m-3 .. m
 #pragma unroll
-  for (int f = 0; f < 5; ++f) mp[f] = bc ? T(0) : mu[f];
-  const T invr = a.rad[rInvR * nr + k], inv_rho0 = a.rad[rInvRho0 * nr + k], rho0 = a.rad[rRho0 * nr + k];
-  const T c2rho0 = a.c2 ? a.c2[((long long)face * nr + k) * P2 + p2] * rho0 : a.rad[rC2Rho0 * nr + k];
-  const T tD = a.met[mD * P2 + p2], tXYD = a.met[mXYD * P2 + p2], tC = a.met[mC * P2 + p2], tXYC = a.met[mXYC * P2 + p2];
-  const T tDivX = a.met[mDivX * P2 + p2], tDivY = a.met[mDivY * P2 + p2], tTX = a.met[mTX * P2 + p2], tTY = a.met[mTY * P2 + p2];
-  // r_vx = -inv_rho0 invr (D dpx + XY/D dpy),  r_ve = -inv_rho0 invr (C dpy + XY/C dpx),  r_vr = -inv_rho0 dpr - rho g0/rho0
-  const T X1 = -invr * inv_rho0 * (tD * mp[kVxi] + tXYC * mp[kVeta]);
-  const T Y1 = -invr * inv_rho0 * (tXYD * mp[kVxi] + tC * mp[kVeta]);
-  const T R1 = -inv_rho0 * mp[kVr];
-  // r_p = -c^2 rho0 div + rho0 g0 v_r ; r_rho = -rho0 div - v_r drho0
-  const T e = -c2rho0 * mp[kP] - rho0 * mp[kRho];
-  const T X2 = invr * tDivX * e, Y2 = invr * tDivY * e, R2 = e;
-  T* I = a.inter;
-  I[inter_vol(g, run, face, 0) + pt] = X1;
-  I[inter_vol(g, run, face, 1) + pt] = Y1;
-  I[inter_vol(g, run, face, 2) + pt] = R1;
-  I[inter_vol(g, run, face, 3) + pt] = X2;
-  I[inter_vol(g, run, face, 4) + pt] = Y2;
-  I[inter_vol(g, run, face, 5) + pt] = R2;
-  const T sig = a.rad[rSigma * nr + k];
-  T pw[5];
-  pw[kRho] = -a.rad[rG0Rho0 * nr + k] * mp[kVr] - sig * mu[kRho];
-  pw[kVxi] = -invr * tTX * e;
-  pw[kVeta] = -invr * tTY * e;
-  pw[kVr] = T(2) * invr * e - a.rad[rDRho0 * nr + k] * mp[kRho] + a.rad[rRho0G0 * nr + k] * mp[kP] - sig * mu[kVr];
-  pw[kP] = -sig * mu[kP];
+  for (int q = 0; q < 7; ++q) { w1[q] = T(0); w2[q] = T(0); }
 #pragma unroll
-  for (int f = 0; f < 5; ++f) {
-    const int s = g.slot[f];
-    if (s < 0) continue;
-    a.lout[g.vol(run, face, s) + pt] = (a.keep ? muq[f] : T(0)) + a.dt * pw[f];
-  }
-  if (a.grad) {
-    const long long gi = (long long)rf * V + l;
-    const T c = sqrt(c2rho0 * inv_rho0);
-    a.grad[gi] += (double)(a.dt * (T(-2) * c * rho0 * a.div[gi]) * mp[kP]);
+  for (int q = 0; q < 4; ++q) { pp[q] = T(0); pv[q] = T(0); }
+  for (int m = kb - 3; m <= ke + 2; ++m) {
+    const bool real = (m >= 0 && m < nr);
+    const bool own = (m >= kb && m < ke);
+    const bool bc = (m == 0 || m == nr - 1);
+    T r1 = T(0), r2 = T(0), part_p = T(0), part_v = T(0);
+    if (real) {
+      const long long o = g.at(m, j, i);
+      const long long plane_c2 = ((long long)face * nr + m) * P2;
+      // ---- every global load of this plane first
+      T lqv[5], lwv[5];
+#pragma unroll
+      for (int f = 0; f < 5; ++f) {
+        const int s = g.slot[f];
+        const bool need = s >= 0 && (own || f == kVr || f == kP || f == kRho);
+        lqv[f] = need ? __ldg(lq + vol(s) + o) : T(0);
+        lwv[f] = need ? __ldg(lw + vol(s) + o) : T(0);
+      }
+      T hx = T(0), hy = T(0), hp = T(0), hr = T(0), hc2 = T(0);
+      const bool do_halo = own && h_in && !bc;
+      if (do_halo) {
+        const long long oh = g.at(m, hgj, hgi);
+        hx = __ldg(lw + vol(sX) + oh) + a.beta * __ldg(lq + vol(sX) + oh);
+        hy = __ldg(lw + vol(sY) + oh) + a.beta * __ldg(lq + vol(sY) + oh);
+        hp = __ldg(lw + vol(sP) + oh) + a.beta * __ldg(lq + vol(sP) + oh);
+        if (sRho >= 0) hr = __ldg(lw + vol(sRho) + oh) + a.beta * __ldg(lq + vol(sRho) + oh);
+        if (a.c2) hc2 = __ldg(a.c2 + plane_c2 + hq2);
+      }
+      const T c2own = a.c2 ? __ldg(a.c2 + plane_c2 + p2) : T(0);
+      const T divv = (own && a.grad) ? __ldg(a.div + plane_c2 + p2) : T(0);
+      const T invr = __ldg(rad + rInvR * nr + m), inv_rho0 = __ldg(rad + rInvRho0 * nr + m);
+      const T rho0 = __ldg(rad + rRho0 * nr + m), c2r = __ldg(rad + rC2Rho0 * nr + m);
+      // ---- compute
+      T mu[5], mp[5];
+#pragma unroll
+      for (int f = 0; f < 5; ++f) {
+        mu[f] = lwv[f] + a.beta * lqv[f];
+        mp[f] = bc ? T(0) : mu[f];
+      }
+      const T c2rho0 = a.c2 ? c2own * rho0 : c2r;
+      const T e = -c2rho0 * mp[kP] - rho0 * mp[kRho];
+      r1 = -inv_rho0 * mp[kVr];
+      r2 = e;
+      if (own) {
+        sX1[ty][tx + 3] = -invr * inv_rho0 * (tD * mp[kVxi] + tXYC * mp[kVeta]);
+        sX2[ty][tx + 3] = invr * tDivX * e;
+        sY1[ty + 3][tx] = -invr * inv_rho0 * (tXYD * mp[kVxi] + tC * mp[kVeta]);
+        sY2[ty + 3][tx] = invr * tDivY * e;
+        if (has_halo) {
+          const T he = -(a.c2 ? hc2 * rho0 : c2r) * hp - rho0 * hr;
+          const T v1 = do_halo ? -invr * inv_rho0 * (hm1 * hx + hm2 * hy) : T(0);
+          const T v2 = do_halo ? invr * hm3 * he : T(0);
+          if (xi_halo) { sX1[hj][hi + 3] = v1; sX2[hj][hi + 3] = v2; }
+          else { sY1[hj + 3][hi] = v1; sY2[hj + 3][hi] = v2; }
+        }
+        // pointwise terms, lw update, gradient
+        const T sig = __ldg(rad + rSigma * nr + m);
+        T pw[5];
+        pw[kRho] = -__ldg(rad + rG0Rho0 * nr + m) * mp[kVr] - sig * mu[kRho];
+        pw[kVxi] = -invr * tTX * e;
+        pw[kVeta] = -invr * tTY * e;
+        pw[kVr] = T(2) * invr * e - __ldg(rad + rDRho0 * nr + m) * mp[kRho] + __ldg(rad + rRho0G0 * nr + m) * mp[kP] -
+                  sig * mu[kVr];
+        pw[kP] = -sig * mu[kP];
+#pragma unroll
+        for (int f = 0; f < 5; ++f) {
+          const int s = g.slot[f];
+          if (s < 0) continue;
+          a.lwout[vol(s) + o] = a.alpha * mu[f];
+          const T base = (a.keep ? lqv[f] : T(0)) + a.dt * pw[f];
+          if (f == kP) part_p = base;
+          else if (f == kVr) part_v = base;
+          else if (f == kRho) a.lout[vol(s) + o] = base;
+          else lqv[f] = base;                                  // v_xi, v_eta: 2-D part added below
+        }
+        if (a.grad) {
+          const T c = sqrt(c2rho0 * inv_rho0);
+          a.grad[plane_c2 + p2] += (double)(a.dt * (T(-2) * c * rho0 * divv) * mp[kP]);
+        }
+        if (m == 1 || m == 2 || m == nr - 3 || m == nr - 2) {
+          const int row = m <= 2 ? m - 1 : m - (nr - 3) + 2;
+          T* rbp = a.rb + (((long long)face * 4 + row) * 2) * P2 + p2;
+          rbp[0] = r1;
+          rbp[P2] = r2;
+        }
+        __syncthreads();
+        const T* x1 = &sX1[ty][tx + 3];
+        const T* x2 = &sX2[ty][tx + 3];
+        const T* y1 = &sY1[ty + 3][tx];
+        const T* y2 = &sY2[ty + 3][tx];
+        const T dx1 = c1 * (x1[1] - x1[-1]) + c2c * (x1[2] - x1[-2]) + c3 * (x1[3] - x1[-3]);
+        const T dx2 = c1 * (x2[1] - x2[-1]) + c2c * (x2[2] - x2[-2]) + c3 * (x2[3] - x2[-3]);
+        const T dy1 = c1 * (y1[TX] - y1[-TX]) + c2c * (y1[2 * TX] - y1[-2 * TX]) + c3 * (y1[3 * TX] - y1[-3 * TX]);
+        const T dy2 = c1 * (y2[TX] - y2[-TX]) + c2c * (y2[2 * TX] - y2[-2 * TX]) + c3 * (y2[3 * TX] - y2[-3 * TX]);
+        const T k2 = -a.dt * a.inv_dxi;
+        part_p += k2 * (dx1 + dy1);
+        a.lout[vol(sX) + o] = lqv[kVxi] + k2 * dx2;
+        a.lout[vol(sY) + o] = lqv[kVeta] + k2 * dy2;
+        // ghost-frame adjoints of the neighbour faces' values (W/E columns, S/N rows)
+        if ((i0 == 0 && tx < 3) || (i0 + TX == n && tx >= TX - 3)) {
+          const bool west = i0 == 0 && tx < 3;
+          const int c = west ? tx : TX + 3 + (tx - (TX - 3));  // x index of the ghost column
+          auto xv = [&](const T* row, int q) { return (q >= 0 && q < XW) ? row[q] : T(0); };
+          const T* r1p = &sX1[ty][0];
+          const T* r2p = &sX2[ty][0];
+          const T f1 = c1 * (xv(r1p, c + 1) - xv(r1p, c - 1)) + c2c * (xv(r1p, c + 2) - xv(r1p, c - 2)) + c3 * (xv(r1p, c + 3) - xv(r1p, c - 3));
+          const T f2 = c1 * (xv(r2p, c + 1) - xv(r2p, c - 1)) + c2c * (xv(r2p, c + 2) - xv(r2p, c - 2)) + c3 * (xv(r2p, c + 3) - xv(r2p, c - 3));
+          const long long og = g.at(m, j, west ? tx - 3 : n + (tx - (TX - 3)));
+          a.lout[vol(sP) + og] = k2 * f1;
+          a.lout[vol(sX) + og] = k2 * f2;
+        }
+        if ((j0 == 0 && ty < 3) || (j0 + TY == n && ty >= TY - 3)) {
+          const bool south = j0 == 0 && ty < 3;
+          const int r = south ? ty : TY + 3 + (ty - (TY - 3));  // y index of the ghost row
+          auto yv = [&](const T (*col)[TX], int q) { return (q >= 0 && q < YH) ? col[q][tx] : T(0); };
+          const T f1 = c1 * (yv(sY1, r + 1) - yv(sY1, r - 1)) + c2c * (yv(sY1, r + 2) - yv(sY1, r - 2)) + c3 * (yv(sY1, r + 3) - yv(sY1, r - 3));
+          const T f2 = c1 * (yv(sY2, r + 1) - yv(sY2, r - 1)) + c2c * (yv(sY2, r + 2) - yv(sY2, r - 2)) + c3 * (yv(sY2, r + 3) - yv(sY2, r - 3));
+          const long long og = g.at(m, south ? ty - 3 : n + (ty - (TY - 3)), i);
+          a.lout[vol(sP) + og] = k2 * f1;
+          a.lout[vol(sY) + og] = k2 * f2;
+        }
+      }
+    }
+    // radial windows and the partial-output ring advance one plane
+    const bool band = real && m >= 3 && m <= nr - 4;
+    const T facr = band ? __ldg(rad + rFacR * nr + m) : T(0);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) { w1[q] = w1[q + 1]; w2[q] = w2[q + 1]; }
+    w1[6] = facr * r1;
+    w2[6] = facr * r2;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) { pp[q] = pp[q + 1]; pv[q] = pv[q + 1]; }
+    pp[3] = part_p;
+    pv[3] = part_v;
+    const int pl = m - 3;
+    if (pl >= kb && pl < ke) {
+      // (Dr^T R)_pl = sum_d a_d facr_{pl-d} R_{pl-d}, a_{-d} = -a_d; window index of pl-d is 3-d
+      const T rp = c1 * (w1[2] - w1[4]) + c2c * (w1[1] - w1[5]) + c3 * (w1[0] - w1[6]);
+      const T rv = c1 * (w2[2] - w2[4]) + c2c * (w2[1] - w2[5]) + c3 * (w2[0] - w2[6]);
+      const long long op = g.at(pl, j, i);
+      a.lout[vol(sP) + op] = pp[0] + a.dt * rp;
+      a.lout[vol(sR) + op] = pv[0] + a.dt * rv;
+    }
+    if (own) __syncthreads();
   }
 }
 
-// Transposed derivatives, on interior points and ghost-frame points.  One thread per
-// (run, face, k, row, column) of the extended face (corners skipped).
+// The one-sided radial rows 1, 2 (onto planes 0..6) and nr-3, nr-2 (onto planes nr-7..nr-1)
+// of the radial transpose, added to p and v_r after adj_stage_kernel.
 template <typename T>
-__global__ void adj_deriv_kernel(const AdjArgs<T> a) {
-  const Geom& g = a.g;
-  const int n = g.n, nr = g.nr, ne = n + 6;
-  const long long E = (long long)ne * ne * nr;
+__global__ void adj_rbdy_kernel(T* lout, const T* rb, const T* rad, Geom g, T dt) {
+  const int n = g.n, nr = g.nr;
+  const long long P2 = (long long)n * n;
   const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= (long long)g.nruns * 6 * E) return;
-  const int rf = idx / E, run = rf / 6, face = rf % 6;
-  const long long l = idx % E;
-  const int i = (int)(l % ne) - 3, j = (int)((l / ne) % ne) - 3, k = (int)(l / ((long long)ne * ne));
-  const bool iin = i >= 0 && i < n, jin = j >= 0 && j < n;
-  if (!iin && !jin) return;                       // corner: never read by a stencil
-  const T* X1 = a.inter + inter_vol(g, run, face, 0);
-  const T* Y1 = a.inter + inter_vol(g, run, face, 1);
-  const T* R1 = a.inter + inter_vol(g, run, face, 2);
-  const T* X2 = a.inter + inter_vol(g, run, face, 3);
-  const T* Y2 = a.inter + inter_vol(g, run, face, 4);
-  const T* R2 = a.inter + inter_vol(g, run, face, 5);
-  auto at = [&](const T* f, int kk, int jj, int ii) -> T {
-    return (ii >= 0 && ii < n && jj >= 0 && jj < n) ? f[g.at(kk, jj, ii)] : T(0);
-  };
-  // -D_xi f and -D_eta f with zero halos (D^T of an antisymmetric stencil)
-  auto mdx = [&](const T* f) {
-    T s = T(0);
-#pragma unroll
-    for (int m = 1; m <= 3; ++m) s += Coef<T>::drp(m) * (at(f, k, j, i + m) - at(f, k, j, i - m));
-    return -a.inv_dxi * s;
-  };
-  auto mdy = [&](const T* f) {
-    T s = T(0);
-#pragma unroll
-    for (int m = 1; m <= 3; ++m) s += Coef<T>::drp(m) * (at(f, k, j + m, i) - at(f, k, j - m, i));
-    return -a.inv_dxi * s;
-  };
-  const long long pt = g.at(k, j, i);
-  const int sP = g.slot[kP], sX = g.slot[kVxi], sY = g.slot[kVeta], sR = g.slot[kVr];
-  if (!iin) {        // W/E ghost columns: adjoints of p and v_xi ghost values
-    a.lout[g.vol(run, face, sP) + pt] = a.dt * mdx(X1);
-    a.lout[g.vol(run, face, sX) + pt] = a.dt * mdx(X2);
-    return;
+  if (idx >= 6 * 14 * P2) return;
+  const int face = (int)(idx / (14 * P2));
+  const int q = (int)((idx / P2) % 14);
+  const int p2 = (int)(idx % P2), i = p2 % n, j = p2 / n;
+  const bool low = q < 7;
+  const int pl = low ? q : nr - 14 + q;                      // planes 0..6 or nr-7..nr-1
+  T s1 = T(0), s2 = T(0);
+  for (int r = 0; r < 2; ++r) {
+    const int kk = low ? 1 + r : nr - 3 + r;
+    const int row = low ? r : 2 + r;
+    const T* rbp = rb + (((long long)face * 4 + row) * 2) * P2 + p2;
+    const T f = rad[rFacR * nr + kk];
+    const T b = low ? Coef<T>::bdy(kk, pl) : -Coef<T>::bdy(nr - 1 - kk, nr - 1 - pl);
+    s1 += f * b * rbp[0];
+    s2 += f * b * rbp[P2];
   }
-  if (!jin) {        // S/N ghost rows: adjoints of p and v_eta ghost values
-    a.lout[g.vol(run, face, sP) + pt] = a.dt * mdy(Y1);
-    a.lout[g.vol(run, face, sY) + pt] = a.dt * mdy(Y2);
-    return;
-  }
-  // radial transpose: (Dr^T f)_k = sum_kk Dr[kk][k] f_kk
-  auto drt = [&](const T* f) {
-    T s = T(0);
-#pragma unroll
-    for (int m = -3; m <= 3; ++m) {
-      const int kk = k - m;                            // row kk reads plane kk + m = k
-      if (m == 0 || kk < 3 || kk > nr - 4) continue;
-      const T cm = m > 0 ? Coef<T>::drp(m) : -Coef<T>::drp(-m);
-      s += a.rad[rFacR * nr + kk] * cm * f[g.at(kk, j, i)];
-    }
-    if (k <= 6)
-      for (int kk = 0; kk < 3; ++kk) s += a.rad[rFacR * nr + kk] * Coef<T>::bdy(kk, k) * f[g.at(kk, j, i)];
-    if (k >= nr - 7)
-      for (int kk = nr - 3; kk < nr; ++kk)
-        s -= a.rad[rFacR * nr + kk] * Coef<T>::bdy(nr - 1 - kk, 6 - (k - (nr - 7))) * f[g.at(kk, j, i)];
-    return s;
-  };
-  a.lout[g.vol(run, face, sP) + pt] += a.dt * (mdx(X1) + mdy(Y1) + drt(R1));
-  a.lout[g.vol(run, face, sX) + pt] += a.dt * mdx(X2);
-  a.lout[g.vol(run, face, sY) + pt] += a.dt * mdy(Y2);
-  a.lout[g.vol(run, face, sR) + pt] += a.dt * drt(R2);
+  const long long o = g.at(pl, j, i);
+  lout[g.vol(0, face, g.slot[kP]) + o] += dt * s1;
+  lout[g.vol(0, face, g.slot[kVr]) + o] += dt * s2;
 }
 
 // Transpose of the edge exchange: every ghost-frame adjoint of buffer `q` is scattered back
 // onto the source lines of the neighbouring face.  mode 0: p scalar + the rotated vector
 // component (v_xi on W/E, v_eta on S/N); mode 1: every stored field scalar.
 template <typename T>
-__global__ void adj_edge_kernel(T* q, const T* ew, const T* eg, const int* s0t, Geom g, int mode) {
+__global__ void adj_edge_kernel(T* q, const T* __restrict__ ew, const T* __restrict__ eg, const int* __restrict__ s0t,
+                                Geom g, int mode) {
+  // grid: x over positions t along the edge, y over (receiving face and edge, layer), z over planes
   const int n = g.n;
-  const long long total = (long long)g.nruns * 24 * 3 * n * g.nr;
-  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= total) return;
-  const int t = idx % n;
-  long long r = idx / n;
-  const int l = r % 3; r /= 3;
-  const int k = r % g.nr; r /= g.nr;
-  const int fe = r % 24, run = (int)(r / 24);
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int fe = blockIdx.y / 3, l = blockIdx.y % 3, k = blockIdx.z, run = 0;
   const int face = fe >> 2, e = fe & 3;
   const EdgeRouteDev rt = cRoute[face][e];
   const bool along_i = rt.src_edge <= 1;
   const int fixed = (rt.src_edge == 0 || rt.src_edge == 2) ? l + 1 : n - 2 - l;
-  const long long crow = ((long long)fe * 3 + l) * 9;
-  const int s0 = s0t[((long long)fe * 3 + l) * n + t];
+  const int crow = (fe * 3 + l) * 9;
+  const int s0 = __ldg(s0t + (fe * 3 + l) * n + t);
   long long dst;
   if (e == 0) dst = g.at(k, -1 - l, t);
   else if (e == 1) dst = g.at(k, n + l, t);
@@ -215,7 +306,8 @@ __global__ void adj_edge_kernel(T* q, const T* ew, const T* eg, const int* s0t, 
     for (int sl = 0; sl < g.nf; ++sl) {
       const T gv = q[g.vol(run, face, sl) + dst];
       T* dstv = q + g.vol(run, rt.src_face, sl);
-      for (int s = 0; s < 9; ++s) atomicAdd(dstv + src_at(s), ew[(crow + s) * n + t] * gv);
+#pragma unroll
+      for (int s = 0; s < 9; ++s) atomicAdd(dstv + src_at(s), __ldg(ew + (crow + s) * n + t) * gv);
     }
     return;
   }
@@ -224,33 +316,42 @@ __global__ void adj_edge_kernel(T* q, const T* ew, const T* eg, const int* s0t, 
   T* pp = q + g.vol(run, rt.src_face, g.slot[kP]);
   T* px = q + g.vol(run, rt.src_face, g.slot[kVxi]);
   T* py = q + g.vol(run, rt.src_face, g.slot[kVeta]);
+#pragma unroll
   for (int s = 0; s < 9; ++s) {
     const long long o = src_at(s);
-    atomicAdd(pp + o, ew[(crow + s) * n + t] * gp);
-    atomicAdd(px + o, eg[((crow + s) * 2 + 0) * n + t] * gv);
-    atomicAdd(py + o, eg[((crow + s) * 2 + 1) * n + t] * gv);
+    atomicAdd(pp + o, __ldg(ew + (crow + s) * n + t) * gp);
+    atomicAdd(px + o, __ldg(eg + ((crow + s) * 2 + 0) * n + t) * gv);
+    atomicAdd(py + o, __ldg(eg + ((crow + s) * 2 + 1) * n + t) * gv);
   }
 }
 
 // FILTER_R^T for every stored field: u_m = sum over output planes k in [5, nr-6] of
-// fr_{|k-m|} lam_k (the end planes of the forward output are constant zeros).
+// fr_{|k-m|} lam_k (the end planes of the forward output are constant zeros).  One thread
+// per (field volume, j, i) column marches the planes with an 11-deep register queue, so
+// lam is read once.
 template <typename T>
 __global__ void adj_filter_r_kernel(const T* lam, T* u, Geom g) {
   const int n = g.n, nr = g.nr;
-  const long long V = (long long)n * n * nr;
+  const long long P = (long long)n * n;
   const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= (long long)g.nruns * 6 * g.nf * V) return;
-  const long long vsel = idx / V;                      // (run*6 + face)*nf + slot
-  const long long l = idx % V;
-  const int i = l % n, j = (l / n) % n, m = l / ((long long)n * n);
-  const T* L = lam + vsel * g.vs;
-  T s = T(0);
-  for (int d = -5; d <= 5; ++d) {
-    const int k = m + d;
-    if (k < 5 || k > nr - 6) continue;
-    s += Coef<T>::filtr(d < 0 ? -d : d) * L[g.at(k, j, i)];
+  if (idx >= (long long)g.nruns * 6 * g.nf * P) return;
+  const long long vsel = idx / P;                      // (run*6 + face)*nf + slot
+  const int p2 = (int)(idx % P), i = p2 % n, j = p2 / n;
+  const T* L = lam + vsel * g.vs + g.at(0, j, i);
+  T* U = u + vsel * g.vs + g.at(0, j, i);
+  auto ld = [&](int k) { return (k >= 5 && k <= nr - 6) ? L[(long long)k * g.plane] : T(0); };
+  T q[11];
+#pragma unroll
+  for (int d = 0; d < 11; ++d) q[d] = ld(d - 5);     // planes m-5 .. m+5 for m = 0
+  for (int m = 0; m < nr; ++m) {
+    T s = Coef<T>::filtr(0) * q[5];
+#pragma unroll
+    for (int d = 1; d <= 5; ++d) s += Coef<T>::filtr(d) * (q[5 - d] + q[5 + d]);
+    U[(long long)m * g.plane] = s;
+#pragma unroll
+    for (int d = 0; d < 10; ++d) q[d] = q[d + 1];
+    q[10] = ld(m + 6);
   }
-  u[vsel * g.vs + g.at(m, j, i)] = s;
 }
 
 // FILTER_ETA^T (dir 1) or FILTER_XI^T (dir 0) with zero halos, evaluated on the interior and
@@ -258,27 +359,28 @@ __global__ void adj_filter_r_kernel(const T* lam, T* u, Geom g) {
 // interior; ghost results are the adjoints of the (unfiltered) halo values and go to
 // `frame`'s frame.
 template <typename T>
-__global__ void adj_filter_dir_kernel(const T* in, T* out, T* frame, Geom g, int dir) {
-  const int n = g.n, nr = g.nr, ne = n + 6;
-  const long long E = (long long)ne * n * nr;          // along-direction extended x other
-  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= (long long)g.nruns * 6 * g.nf * E) return;
-  const long long vsel = idx / E;
-  const long long l = idx % E;
-  const int a_ = (int)(l % ne) - 3;                     // position along the filter direction
-  const int b_ = (int)((l / ne) % n);                   // the other in-face coordinate
-  const int k = (int)(l / ((long long)ne * n));
-  const T* f = in + vsel * g.vs;
+__global__ void adj_filter_dir_kernel(const T* __restrict__ in, T* out, T* frame, Geom g, int dir) {
+  // grid: x over the points of a row (n + 6 extended columns for xi, n for eta), y over rows
+  // (n for xi, n + 6 extended rows for eta), z over (field volume, plane)
+  const int n = g.n;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= (dir ? n : n + 6)) return;
+  const int k = blockIdx.z % g.nr;
+  const long long vbase = (long long)(blockIdx.z / g.nr) * g.vs;
+  const int a_ = dir ? y - 3 : x - 3;                     // along the filter direction
+  const int b_ = dir ? x : y;                             // the other in-face coordinate
+  const T* f = in + vbase;
   auto val = [&](int aa) -> T {
     if (aa < 0 || aa >= n) return T(0);
-    return dir ? f[g.at(k, aa, b_)] : f[g.at(k, b_, aa)];
+    return __ldg(dir ? f + g.at(k, aa, b_) : f + g.at(k, b_, aa));
   };
   T s = Coef<T>::filt(0) * val(a_);
 #pragma unroll
   for (int m = 1; m <= 3; ++m) s += Coef<T>::filt(m) * (val(a_ - m) + val(a_ + m));
   const long long pt = dir ? g.at(k, a_, b_) : g.at(k, b_, a_);
-  if (a_ >= 0 && a_ < n) out[vsel * g.vs + pt] = s;
-  else frame[vsel * g.vs + pt] = s;
+  if (a_ >= 0 && a_ < n) out[vbase + pt] = s;
+  else frame[vbase + pt] = s;
 }
 
 // Receivers: p sampled with trilinear weights over the 8 grid points around each receiver

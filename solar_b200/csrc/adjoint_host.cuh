@@ -25,6 +25,7 @@ static int adj_alloc(solar_ctx* c) {
   if (cudaMalloc(&b.I, Ib) != cudaSuccess) { cudaGetLastError(); return fail(SOLAR_ERR_NOMEM, "adjoint buffers: out of device memory"); }
   CK(cudaMemsetAsync(b.I, 0, Ib, c->stream));
   CK(cudaMalloc((void**)&b.grad, (size_t)6 * vol_compact(c) * sizeof(double)));
+  CK(cudaMalloc(&b.rb, (size_t)6 * 4 * 2 * c->g.n * c->g.n * c->esize));
   return SOLAR_OK;
 }
 
@@ -43,12 +44,13 @@ static int adj_reserve(void** p, size_t* have, size_t want) {
 }
 
 template <typename T>
-static AdjArgs<T> adj_args(solar_ctx* c, double dt) {
-  AdjArgs<T> a;
-  a.lq = (const T*)c->adj.L;
-  a.lw = (T*)c->adj.LW;
-  a.lout = (T*)c->adj.L;
-  a.inter = (T*)c->adj.I;
+static AdjStageArgs<T> adj_args(solar_ctx* c, double dt) {
+  AdjStageArgs<T> a;
+  a.lq = nullptr;
+  a.lw = nullptr;
+  a.lout = nullptr;
+  a.lwout = nullptr;
+  a.rb = nullptr;
   a.div = nullptr;
   a.c2 = (const T*)c->dt.c2;
   a.grad = nullptr;
@@ -60,23 +62,41 @@ static AdjArgs<T> adj_args(solar_ctx* c, double dt) {
   a.dt = (T)dt;
   a.inv_dxi = (T)(1.0 / c->ht.dxi);
   a.keep = 0;
+  a.kchunk = 0;
   return a;
 }
 
 static unsigned blocks_for(long long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
-// L^T applied to buffer L (plus the pointwise and RK parts selected by `a`), then the
-// transposed edge exchange.
+// L^T applied to buffer L (plus the pointwise and RK parts selected by `a`): the fused
+// transposed stage writes lambda_q and lambda_w to the partner buffers T1, T2 (inputs'
+// halos are read by neighbouring CTAs), the one-sided radial rows are added, the ghost
+// adjoints are scattered back, and the buffer pairs swap roles.
 template <typename T>
-static int enqueue_rhs_adjoint(solar_ctx* c, const AdjArgs<T>& a) {
+static int enqueue_rhs_adjoint(solar_ctx* c, AdjStageArgs<T> a) {
+  AdjBuffers& b = c->adj;
   const Geom& g = c->g;
-  const long long V = vol_compact(c);
-  const long long E = (long long)(g.n + 6) * (g.n + 6) * g.nr;
-  adj_pre_kernel<T><<<blocks_for(6 * V, 256), 256, 0, c->stream>>>(a);
-  adj_deriv_kernel<T><<<blocks_for(6 * E, 256), 256, 0, c->stream>>>(a);
-  adj_edge_kernel<T><<<blocks_for(24LL * 3 * g.n * g.nr, 128), 128, 0, c->stream>>>(
-      (T*)c->adj.L, (const T*)c->dt.ew, (const T*)c->dt.eg, c->dt.s0t, g, 0);
+  a.lq = (const T*)b.L;
+  a.lw = (const T*)b.LW;
+  a.lout = (T*)b.T1;
+  a.lwout = (T*)b.T2;
+  a.rb = (T*)b.rb;
+  const bool wide = g.n % 32 == 0;
+  const int tx = wide ? 32 : 16, ty = wide ? 8 : 16;
+  const long long tiles = 6LL * (g.n / tx) * (g.n / ty);
+  const long long want = 148LL * 6;
+  const int nch = (int)std::max<long long>(1, (want + tiles - 1) / tiles);
+  a.kchunk = std::max(8, (g.nr + nch - 1) / nch);
+  dim3 grid((unsigned)((g.n / tx) * (g.n / ty)), (unsigned)((g.nr + a.kchunk - 1) / a.kchunk), 6);
+  if (wide) adj_stage_kernel<T, 32, 8><<<grid, 256, 0, c->stream>>>(a);
+  else adj_stage_kernel<T, 16, 16><<<grid, 256, 0, c->stream>>>(a);
+  adj_rbdy_kernel<T><<<blocks_for(6LL * 14 * g.n * g.n, 256), 256, 0, c->stream>>>((T*)b.T1, (const T*)b.rb,
+                                                                                   (const T*)c->dt.rad, g, a.dt);
+  adj_edge_kernel<T><<<dim3(blocks_for(g.n, 128), 72, g.nr), 128, 0, c->stream>>>(
+      (T*)b.T1, (const T*)c->dt.ew, (const T*)c->dt.eg, c->dt.s0t, g, 0);
   CK(cudaGetLastError());
+  std::swap(b.L, b.T1);
+  std::swap(b.LW, b.T2);
   return SOLAR_OK;
 }
 
@@ -84,15 +104,14 @@ static int enqueue_rhs_adjoint(solar_ctx* c, const AdjArgs<T>& a) {
 template <typename T>
 static int enqueue_filter_adjoint(solar_ctx* c) {
   const Geom& g = c->g;
-  const long long V = vol_compact(c);
-  const long long Ed = (long long)(g.n + 6) * g.n * g.nr;
   T* L = (T*)c->adj.L;
   T* T1 = (T*)c->adj.T1;
   T* T2 = (T*)c->adj.T2;
-  adj_filter_r_kernel<T><<<blocks_for(6LL * g.nf * V, 256), 256, 0, c->stream>>>(L, T1, g);
-  adj_filter_dir_kernel<T><<<blocks_for(6LL * g.nf * Ed, 256), 256, 0, c->stream>>>(T1, T2, L, g, 1);
-  adj_filter_dir_kernel<T><<<blocks_for(6LL * g.nf * Ed, 256), 256, 0, c->stream>>>(T2, L, L, g, 0);
-  adj_edge_kernel<T><<<blocks_for(24LL * 3 * g.n * g.nr, 128), 128, 0, c->stream>>>(
+  adj_filter_r_kernel<T><<<blocks_for(6LL * g.nf * g.n * g.n, 128), 128, 0, c->stream>>>(L, T1, g);
+  const unsigned zvol = (unsigned)(6 * g.nf * g.nr);
+  adj_filter_dir_kernel<T><<<dim3(blocks_for(g.n, 128), g.n + 6, zvol), 128, 0, c->stream>>>(T1, T2, L, g, 1);
+  adj_filter_dir_kernel<T><<<dim3(blocks_for(g.n + 6, 128), g.n, zvol), 128, 0, c->stream>>>(T2, L, L, g, 0);
+  adj_edge_kernel<T><<<dim3(blocks_for(g.n, 128), 72, g.nr), 128, 0, c->stream>>>(
       L, (const T*)c->dt.ew, (const T*)c->dt.eg, c->dt.s0t, g, 1);
   CK(cudaGetLastError());
   return SOLAR_OK;
@@ -107,7 +126,7 @@ static int enqueue_step_adjoint(solar_ctx* c, const T* dstep, double* grad) {
   CK(cudaMemsetAsync(c->adj.LW, 0, (size_t)state_bytes(c), c->stream));
   const long long V6 = 6 * vol_compact(c);
   for (int s = 4; s >= 0; --s) {
-    AdjArgs<T> a = adj_args<T>(c, c->desc.dt);
+    AdjStageArgs<T> a = adj_args<T>(c, c->desc.dt);
     a.alpha = s == 0 ? T(0) : (T)kAlpha[s];
     a.beta = (T)kBeta[s];
     a.keep = 1;

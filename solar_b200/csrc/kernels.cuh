@@ -132,8 +132,13 @@ struct EdgeArgs {
 // once, so the planes' tap sums run in parallel.  Coefficient tables are stored
 // position-fastest ([face][edge][layer][tap][position]) so every table load of a warp is
 // one contiguous segment.
+// Resident CTAs per SM the compiler budgets registers for: the kernel is latency-bound,
+// so float with at most 2 planes per CTA is held to 64 registers (measured faster); double
+// and 4-plane float keep their registers (a tighter budget spills).
+template <typename T, int KC> struct EdgeMinBlocks { static constexpr int value = (sizeof(T) == 4 && KC <= 2) ? 8 : 1; };
+
 template <typename T, int KC>
-__global__ void __launch_bounds__(128) edge_kernel(const EdgeArgs<T> a) {
+__global__ void __launch_bounds__(128, (EdgeMinBlocks<T, KC>::value)) edge_kernel(const EdgeArgs<T> a) {
   extern __shared__ __align__(16) unsigned char esm[];
   T* buf = reinterpret_cast<T*>(esm);                    // [field][kk][layer][t_s]
   const Geom& g = a.g;
@@ -161,12 +166,25 @@ __global__ void __launch_bounds__(128) edge_kernel(const EdgeArgs<T> a) {
         const T* rowp = src + (long long)(JOFF + (low ? l + 1 : n - 2 - l)) * g.pitch + IOFF;
         cp_async_16(dst + idx, rowp + t);
       }
-    } else {                                             // columns: the three layers of a row together
-      for (int idx = threadIdx.x; idx < 3 * n; idx += blockDim.x) {
-        const int t = idx / 3, l = idx - 3 * t;
-        const int col = low ? l + 1 : n - 2 - l;
-        cp_async_small<sizeof(T)>(dst + l * n + t, src + (long long)(JOFF + t) * g.pitch + IOFF + col);
-      }
+    }
+  }
+  if (!along_i) {
+    // columns: the three layers of a row lie in one aligned 4-value group (columns 0..3 or
+    // n-4..n-1), fetched as 16-byte vectors and spread to the [layer][t] layout
+    const int c0 = low ? 0 : n - 4;
+    constexpr int W16 = 16 / sizeof(T);
+#pragma unroll 4
+    for (int idx = threadIdx.x; idx < nfl * kc * n; idx += blockDim.x) {
+      const int fk = idx / n, t = idx - fk * n;
+      const int f = fk / kc, kk = fk - f * kc;
+      const T* rp = a.q + g.vol(run, rt.src_face, slot_of(f)) + (long long)(kb + kk) * g.plane +
+                    (long long)(JOFF + t) * g.pitch + IOFF + c0;
+      T v[4];
+      ldv(rp, v);
+      if (W16 == 2) ldv(rp + 2, v + 2);
+      T* dst = buf + (long long)(f * KC + kk) * 3 * n;
+#pragma unroll
+      for (int l = 0; l < 3; ++l) dst[l * n + t] = v[low ? 1 + l : 2 - l];
     }
   }
   cp_async_wait_all();

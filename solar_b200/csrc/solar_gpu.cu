@@ -62,7 +62,8 @@ struct AdjBuffers {
   void* LW = nullptr;       // lambda_w
   void* T1 = nullptr;       // filter-transpose scratch
   void* T2 = nullptr;
-  void* I = nullptr;        // six intermediate volumes per face
+  void* I = nullptr;        // stage-kernel output scratch of the recomputation (divergence)
+  void* rb = nullptr;       // R1, R2 of the one-sided radial rows (planes 1, 2, nr-3, nr-2)
   double* grad = nullptr;   // dJ/dc, compact [face][k][j][i]
   void* ckpt = nullptr;     // state checkpoints (padded copies of the state buffer)
   size_t ckpt_bytes = 0;
@@ -181,7 +182,34 @@ static bool make_map(const solar_ctx* c, const void* base, int bx, int by, CUten
   return r == CUDA_SUCCESS;
 }
 
-constexpr int kEdgePlanes = 4;   // radial planes per edge-kernel CTA
+// Radial planes per edge-kernel CTA.  0 = choose from the grid size.
+#ifndef SOLAR_EDGE_PLANES
+#define SOLAR_EDGE_PLANES 0
+#endif
+
+template <typename T, int KC>
+static int launch_edge_kc(solar_ctx* c, const EdgeArgs<T>& a, int mode) {
+  const int nfl = mode == 1 ? c->g.nf : 3;
+  const size_t smem = (size_t)nfl * KC * 3 * c->g.n * sizeof(T);
+  if (smem > 48 * 1024) {
+    static bool attr_set = false;
+    if (!attr_set) {
+      CK(cudaFuncSetAttribute(edge_kernel<T, KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+      attr_set = true;
+    }
+  }
+  dim3 grid((c->g.nr + KC - 1) / KC, 4 * c->g.nface, c->g.nruns);
+  edge_kernel<T, KC><<<grid, 128, smem, c->stream>>>(a);
+  return SOLAR_OK;
+}
+
+static int edge_planes(const solar_ctx* c) {
+  if (SOLAR_EDGE_PLANES > 0) return SOLAR_EDGE_PLANES;
+  const long long ctas4 = 4LL * c->g.nface * c->g.nruns * ((c->g.nr + 3) / 4);
+  if (ctas4 >= 148LL * 8) return 4;
+  if (2 * ctas4 >= 148LL * 8) return 2;
+  return 1;
+}
 
 template <typename T>
 static int launch_edge(solar_ctx* c, void* buf, int mode, const int* active) {
@@ -193,18 +221,11 @@ static int launch_edge(solar_ctx* c, void* buf, int mode, const int* active) {
   a.active = active;
   a.g = c->g;
   a.mode = mode;
-  const int nfl = mode == 1 ? c->g.nf : 3;
-  const size_t smem = (size_t)nfl * kEdgePlanes * 3 * c->g.n * sizeof(T);
-  if (smem > 48 * 1024) {
-    static bool attr_set = false;
-    if (!attr_set) {
-      CK(cudaFuncSetAttribute(edge_kernel<T, kEdgePlanes>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-      attr_set = true;
-    }
+  switch (edge_planes(c)) {
+    case 1: return launch_edge_kc<T, 1>(c, a, mode);
+    case 2: return launch_edge_kc<T, 2>(c, a, mode);
+    default: return launch_edge_kc<T, 4>(c, a, mode);
   }
-  dim3 grid((c->g.nr + kEdgePlanes - 1) / kEdgePlanes, 4 * c->g.nface, c->g.nruns);
-  edge_kernel<T, kEdgePlanes><<<grid, 128, smem, c->stream>>>(a);
-  return SOLAR_OK;
 }
 
 template <typename T, int TX, int TY, int MODE, bool HAS_RHO>
@@ -492,7 +513,7 @@ int solar_gpu_finalize(solar_ctx* c) {
                   c->dt.rad64, c->dt.vol2, c->dt.drw, c->dt.c2_64, c->dt.tanx, c->dt.gr};
   for (void* p : ptrs)
     if (p) cudaFree(p);
-  void* aptrs[] = {c->adj.L, c->adj.LW, c->adj.T1, c->adj.T2, c->adj.I, c->adj.grad, c->adj.ckpt,
+  void* aptrs[] = {c->adj.L, c->adj.LW, c->adj.T1, c->adj.T2, c->adj.I, c->adj.rb, c->adj.grad, c->adj.ckpt,
                    c->adj.div, c->adj.traces, c->adj.rec_off, c->adj.rec_w, c->split_items, c->split_slots};
   for (void* p : aptrs)
     if (p) cudaFree(p);
