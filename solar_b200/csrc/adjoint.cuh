@@ -402,16 +402,4 @@ __global__ void inject_kernel(T* lam, const long long* rec_off, const double* re
   for (int c = 0; c < 8; ++c) atomicAdd(lam + rec_off[r * 8 + c], (T)(rec_w[r * 8 + c] * res[r]));
 }
 
-// One slot of a padded buffer (run 0, all faces) -> compact [face][k][j][i].
-template <typename T>
-__global__ void gather_slot_kernel(const T* buf, int slot, T* dst, Geom g) {
-  const long long V = (long long)g.n * g.n * g.nr;
-  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= 6 * V) return;
-  const int face = idx / V;
-  const long long l = idx % V;
-  const int i = l % g.n, j = (l / g.n) % g.n, k = l / ((long long)g.n * g.n);
-  dst[idx] = buf[g.vol(0, face, slot) + g.at(k, j, i)];
-}
-
 }  // namespace solar

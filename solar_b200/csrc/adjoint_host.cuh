@@ -21,9 +21,6 @@ static int adj_alloc(solar_ctx* c) {
     if (cudaMalloc(p, S) != cudaSuccess) { cudaGetLastError(); return fail(SOLAR_ERR_NOMEM, "adjoint buffers: out of device memory"); }
     CK(cudaMemsetAsync(*p, 0, S, c->stream));
   }
-  const size_t Ib = (size_t)36 * c->g.vs * c->esize;   // six intermediate volumes per face
-  if (cudaMalloc(&b.I, Ib) != cudaSuccess) { cudaGetLastError(); return fail(SOLAR_ERR_NOMEM, "adjoint buffers: out of device memory"); }
-  CK(cudaMemsetAsync(b.I, 0, Ib, c->stream));
   CK(cudaMalloc((void**)&b.grad, (size_t)6 * vol_compact(c) * sizeof(double)));
   CK(cudaMalloc(&b.rb, (size_t)6 * 4 * 2 * c->g.n * c->g.n * c->esize));
   return SOLAR_OK;
@@ -145,10 +142,7 @@ static int enqueue_step_div(solar_ctx* c, T* dstep) {
   int cur = 0, rc;
   for (int s = 0; s < 5; ++s) {
     if ((rc = launch_edge<T>(c, bufs[cur], 0, nullptr))) return rc;
-    if ((rc = launch_stage<T>(c, bufs[cur], c->adj.I, 3, s, nullptr))) return rc;
-    gather_slot_kernel<T><<<blocks_for(V6, 256), 256, 0, c->stream>>>((const T*)c->adj.I, c->g.slot[kP],
-                                                                       dstep + s * V6, c->g);
-    if ((rc = launch_stage<T>(c, bufs[cur], bufs[cur ^ 1], s == 0 ? 1 : 0, s, nullptr))) return rc;
+    if ((rc = launch_stage<T>(c, bufs[cur], bufs[cur ^ 1], s == 0 ? 4 : 5, s, nullptr, dstep + s * V6))) return rc;
     cur ^= 1;
   }
   if ((rc = launch_edge<T>(c, bufs[cur], 1, nullptr))) return rc;

@@ -302,7 +302,9 @@ enum { mD = 0, mXYD, mC, mXYC, mDivX, mDivY, mTX, mTY, mVol, mCount };
 // Tam-Dong one-sided rows apply (derivative.f90:704-754).
 // MODE 0: RK update, stages 2-5 (reads qw).  MODE 1: RK update, stage 1 (qw = 0).
 // MODE 2: write the raw COMPUTE_RHS into qout.  MODE 3: write (grad_xi, grad_eta,
-// grad_r, div) into the v_xi, v_eta, v_r, p slots of qout.
+// grad_r, div) into the v_xi, v_eta, v_r, p slots of qout.  MODE 4 / 5: MODE 1 / 0 that
+// also store the divergence of the stage input (compact, run 0) into divout -- the
+// forward recomputation of the adjoint.
 constexpr int kLead = 7;
 // tile-ring depth: plane k is computed while planes k+1, k+2 are in flight
 template <typename T> struct TileRing { static constexpr int value = 3; };
@@ -319,6 +321,7 @@ struct StageArgs {
   const T* rad;             // [kNumRadial][nr]
   const T* met;             // [kNumMetric][n][n]
   const T* c2;              // optional compact c^2 [face][k][j][i] (run-shared) or nullptr
+  T* divout;                // MODE 4/5: compact divergence [face][k][j][i]
   const int* active;
   int* err;
   Geom g;
@@ -343,8 +346,10 @@ struct StageLayout {
 
 // Each thread owns V consecutive points of one row (V = 16 bytes / sizeof(T)), so the
 // CTA has (TX/V) x TY threads and every shared-memory access is a 16-byte vector.
-template <typename T, int TX, int TY, int MODE, bool HAS_RHO>
+template <typename T, int TX, int TY, int MODE_, bool HAS_RHO>
 __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __grid_constant__ StageArgs<T> a) {
+  constexpr bool STORE_DIV = MODE_ >= 4;
+  constexpr int MODE = MODE_ == 4 ? 1 : (MODE_ == 5 ? 0 : MODE_);
   constexpr int V = Vec16<T>::V;
   constexpr int kTile = TileRing<T>::value;
   constexpr int NT = TX / V;
@@ -512,7 +517,7 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __
     const int offk = k - ks;
     const int brow = k < 3 ? k : nr - 1 - k;
     T r_p[V], r_vx[V], r_ve[V], r_vr[V], r_rho[V], vr[V], pv[V], vxv[V];
-    T o0[V], o1[V], o2[V], o3[V];
+    T o0[V], o1[V], o2[V], o3[V], dvv[V];
 #pragma unroll
     for (int q = 0; q < V; ++q) {
       const T dpx = a.inv_dxi * (c1 * (wp[5 + q] - wp[3 + q]) + c2 * (wp[6 + q] - wp[2 + q]) + c3 * (wp[7 + q] - wp[1 + q]));
@@ -544,6 +549,7 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __
       const T geta = invr * (m_C[q] * dpy + m_XYC[q] * dpx);
       const T div = invr * (m_DivX[q] * dvx + m_DivY[q] * dvy - m_TX[q] * vxi - m_TY[q] * veta) + dvr + T(2) * v_r * invr;
       vr[q] = v_r; pv[q] = p; vxv[q] = vxi;
+      if (STORE_DIV) dvv[q] = div;
       if (MODE == 3) {
         o0[q] = gxi; o1[q] = geta; o2[q] = dpr; o3[q] = div;
       } else {
@@ -561,6 +567,7 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __
       }
     }
     const long long kp = (long long)k * g.plane;
+    if (STORE_DIV) stv(a.divout + ((long long)face * nr + k) * P2 + p2, dvv);
     if (MODE == 3) {
       stv(outS[kVxi] + kp, o0);
       stv(outS[kVeta] + kp, o1);

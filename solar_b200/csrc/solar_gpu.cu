@@ -62,7 +62,6 @@ struct AdjBuffers {
   void* LW = nullptr;       // lambda_w
   void* T1 = nullptr;       // filter-transpose scratch
   void* T2 = nullptr;
-  void* I = nullptr;        // stage-kernel output scratch of the recomputation (divergence)
   void* rb = nullptr;       // R1, R2 of the one-sided radial rows (planes 1, 2, nr-3, nr-2)
   double* grad = nullptr;   // dJ/dc, compact [face][k][j][i]
   void* ckpt = nullptr;     // state checkpoints (padded copies of the state buffer)
@@ -254,7 +253,9 @@ static int launch_stage_mode(solar_ctx* c, StageArgs<T>& a, const void* qin, int
     case 0: return rho ? launch_stage_t<T, TX, TY, 0, true>(c, a, qin) : launch_stage_t<T, TX, TY, 0, false>(c, a, qin);
     case 1: return rho ? launch_stage_t<T, TX, TY, 1, true>(c, a, qin) : launch_stage_t<T, TX, TY, 1, false>(c, a, qin);
     case 2: return rho ? launch_stage_t<T, TX, TY, 2, true>(c, a, qin) : launch_stage_t<T, TX, TY, 2, false>(c, a, qin);
-    default: return rho ? launch_stage_t<T, TX, TY, 3, true>(c, a, qin) : launch_stage_t<T, TX, TY, 3, false>(c, a, qin);
+    case 3: return rho ? launch_stage_t<T, TX, TY, 3, true>(c, a, qin) : launch_stage_t<T, TX, TY, 3, false>(c, a, qin);
+    case 4: return rho ? launch_stage_t<T, TX, TY, 4, true>(c, a, qin) : launch_stage_t<T, TX, TY, 4, false>(c, a, qin);
+    default: return rho ? launch_stage_t<T, TX, TY, 5, true>(c, a, qin) : launch_stage_t<T, TX, TY, 5, false>(c, a, qin);
   }
 }
 
@@ -268,8 +269,9 @@ static void default_tile(int n, bool fp32, int* tx, int* ty) {
 
 template <typename T>
 static int launch_stage(solar_ctx* c, const void* qin, void* qout, int mode, int stage,
-                        const int* active) {
+                        const int* active, void* divout = nullptr) {
   StageArgs<T> a;
+  a.divout = (T*)divout;
   a.qout = (T*)qout;
   a.qw = (T*)c->W;
   a.rad = (const T*)c->dt.rad;
@@ -284,7 +286,7 @@ static int launch_stage(solar_ctx* c, const void* qin, void* qout, int mode, int
   a.inv_dxi = (T)(1.0 / c->ht.dxi);
   a.kchunk = c->kchunk;
   int tx = c->tile_x, ty = c->tile_y;
-  if (mode >= 2) default_tile(c->g.n, c->fp32, &tx, &ty);   // operator-level calls
+  if (mode == 2 || mode == 3) default_tile(c->g.n, c->fp32, &tx, &ty);   // operator-level calls
   if (tx == 16 && ty == 16) return launch_stage_mode<T, 16, 16>(c, a, qin, mode);
   if (tx == 32 && ty == 8) return launch_stage_mode<T, 32, 8>(c, a, qin, mode);
   if (tx == 32 && ty == 16) return launch_stage_mode<T, 32, 16>(c, a, qin, mode);
@@ -513,7 +515,7 @@ int solar_gpu_finalize(solar_ctx* c) {
                   c->dt.rad64, c->dt.vol2, c->dt.drw, c->dt.c2_64, c->dt.tanx, c->dt.gr};
   for (void* p : ptrs)
     if (p) cudaFree(p);
-  void* aptrs[] = {c->adj.L, c->adj.LW, c->adj.T1, c->adj.T2, c->adj.I, c->adj.rb, c->adj.grad, c->adj.ckpt,
+  void* aptrs[] = {c->adj.L, c->adj.LW, c->adj.T1, c->adj.T2, c->adj.rb, c->adj.grad, c->adj.ckpt,
                    c->adj.div, c->adj.traces, c->adj.rec_off, c->adj.rec_w, c->split_items, c->split_slots};
   for (void* p : aptrs)
     if (p) cudaFree(p);
