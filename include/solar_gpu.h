@@ -196,6 +196,37 @@ void* solar_gpu_stream(solar_ctx* c);
  * out5 = (sum of field^2 (field 1..5; 0 = none), energy, mass, max |p|, non-finite count). */
 int solar_gpu_reduce_owned(solar_ctx* c, int run, int field, double* out5);
 
+/* ---- The reference's output files (output.f90), for the zones of run `run` ------------
+ * Paths are relative to `dir` (the reference writes into its working directory); missing
+ * directories are created.  Zone z (0-based) is the reference's rank z and zone z+1 of the
+ * px = py = pr = 1 layout.  NNN is the three-digit cue (dirs.c:20).
+ *   restart  WRITE_RESTART (output.f90:86-190): dir/Restart/restart.NNN.<z+1>, a 28-byte
+ *            header (int32 nx, ny, nr, 5; float64 time; int32 step) then q(nx,ny,nr,5)
+ *            float64 in Fortran order.  The reference has no reader; solar_gpu_read_restart
+ *            loads the same files into the state (header checked against the context).
+ *   visual   WRITE_VISUAL (output.f90:192-240): dir/Visual/NNN/vis_<z>, one Fortran
+ *            unformatted record (4-byte length markers) of q(:,:,o_rad,1:5).
+ *   grid     WRITE_GRID (output.f90:242-267): dir/Visual/grid/grid_<z>, FORMAT(1x,7i5).
+ *   trace    WRITE_RADIAL_TRACE (output.f90:309-343): appends ((q(1,1,k,l),k=1,nr),l=1,5)
+ *            to dir/trace_<z+1> with FORMAT(1x,5(ES13.5)). */
+int solar_gpu_write_restart(solar_ctx* c, int run, const char* dir, int cue, double time, int step);
+int solar_gpu_read_restart(solar_ctx* c, int run, const char* dir, int cue, double* time, int* step);
+int solar_gpu_write_visual(solar_ctx* c, int run, const char* dir, int cue);
+int solar_gpu_write_grid(solar_ctx* c, const char* dir);
+int solar_gpu_write_radial_trace(solar_ctx* c, int run, const char* dir);
+
+/* o_rad of SOLAR_DATA (ic_acoustic_wave.f90:124-132), 0-based: the plane WRITE_VISUAL dumps. */
+int solar_gpu_output_plane(solar_ctx* c, int* k);
+
+/* The same formats for one zone from host arrays (no device needed). */
+int solar_io_cue_name(int cue, char* buf, int len);
+int solar_io_format_es(double v, int w, int d, char* out);          /* Fortran ESw.d, out: w+1 chars */
+int solar_io_write_restart(const char* path, const double* q, int nx, int ny, int nr, double time, int step);
+int solar_io_read_restart(const char* path, double* q, int nx, int ny, int nr, double* time, int* step);
+int solar_io_write_visual(const char* path, const double* plane5, int nx, int ny);
+int solar_io_write_grid(const char* path, const int* seven);
+int solar_io_append_trace(const char* path, const double* values, int count);
+
 /* ---- Discrete adjoint (run 0 of a context with nruns == 1) -------------------------
  * No counterpart in the reference, which has no adjoint.  These are the exact transposes
  * of the discrete forward operators above: COMPUTE_RHS + BC_RHS + SPONGE, FILTER_EXP

@@ -84,6 +84,19 @@ EXPORTS = {
     "solar_gpu_unpack_lines": [_P, ctypes.c_int, _I, ctypes.c_int, ctypes.c_void_p],
     "solar_gpu_stream": [_P],
     "solar_gpu_reduce_owned": [_P, ctypes.c_int, ctypes.c_int, _D],
+    "solar_gpu_write_restart": [_P, ctypes.c_int, ctypes.c_char_p, ctypes.c_int, ctypes.c_double, ctypes.c_int],
+    "solar_gpu_read_restart": [_P, ctypes.c_int, ctypes.c_char_p, ctypes.c_int, _D, _I],
+    "solar_gpu_write_visual": [_P, ctypes.c_int, ctypes.c_char_p, ctypes.c_int],
+    "solar_gpu_write_grid": [_P, ctypes.c_char_p],
+    "solar_gpu_write_radial_trace": [_P, ctypes.c_int, ctypes.c_char_p],
+    "solar_gpu_output_plane": [_P, _I],
+    "solar_io_cue_name": [ctypes.c_int, ctypes.c_char_p, ctypes.c_int],
+    "solar_io_format_es": [ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_char_p],
+    "solar_io_write_restart": [ctypes.c_char_p, _D, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int],
+    "solar_io_read_restart": [ctypes.c_char_p, _D, ctypes.c_int, ctypes.c_int, ctypes.c_int, _D, _I],
+    "solar_io_write_visual": [ctypes.c_char_p, _D, ctypes.c_int, ctypes.c_int],
+    "solar_io_write_grid": [ctypes.c_char_p, _I],
+    "solar_io_append_trace": [ctypes.c_char_p, _D, ctypes.c_int],
 }
 
 # entry points whose return type is not int

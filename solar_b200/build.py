@@ -16,9 +16,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsolar_gpu.so")
-SOURCES = [os.path.join(CSRC, "solar_gpu.cu"), os.path.join(CSRC, "noalloc.cu"), os.path.join(CSRC, "tables.cpp")]
-HEADERS = [os.path.join(CSRC, "kernels.cuh"), os.path.join(CSRC, "tma.cuh"), os.path.join(CSRC, "tables.h"),
-           os.path.join(ROOT, "include", "solar_gpu.h")]
+SOURCES = [os.path.join(CSRC, "solar_gpu.cu"), os.path.join(CSRC, "noalloc.cu"), os.path.join(CSRC, "tables.cpp"),
+           os.path.join(CSRC, "io.cpp")]
+HEADERS = [os.path.join(CSRC, h) for h in ("kernels.cuh", "tma.cuh", "tables.h", "adjoint.cuh", "adjoint_host.cuh",
+                                            "split_host.cuh", "io_host.cuh")] + [os.path.join(ROOT, "include", "solar_gpu.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -884,3 +884,4 @@ int solar_gpu_synchronize(solar_ctx* c) {
 
 #include "adjoint_host.cuh"
 #include "split_host.cuh"
+#include "io_host.cuh"

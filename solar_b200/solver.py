@@ -203,6 +203,34 @@ class Solver:
     def synchronize(self) -> None:
         _lib.check(self.lib.solar_gpu_synchronize(self._h))
 
+    # ------------------------------------------------------------------ output files
+    def write_restart(self, dir: str, cue: int, time: float, step: int, run: int = 0) -> None:
+        """WRITE_RESTART (output.f90:86-190) for the six zones of `run`."""
+        _lib.check(self.lib.solar_gpu_write_restart(self._h, run, dir.encode(), int(cue), float(time), int(step)))
+
+    def read_restart(self, dir: str, cue: int, run: int = 0):
+        """Load the six restart files of `cue` into the state; returns (time, step)."""
+        t, s = ctypes.c_double(), ctypes.c_int()
+        _lib.check(self.lib.solar_gpu_read_restart(self._h, run, dir.encode(), int(cue), ctypes.byref(t), ctypes.byref(s)))
+        return t.value, s.value
+
+    def write_visual(self, dir: str, cue: int, run: int = 0) -> None:
+        """WRITE_VISUAL (output.f90:192-240): plane o_rad of every zone."""
+        _lib.check(self.lib.solar_gpu_write_visual(self._h, run, dir.encode(), int(cue)))
+
+    def write_grid(self, dir: str) -> None:
+        """WRITE_GRID (output.f90:242-267)."""
+        _lib.check(self.lib.solar_gpu_write_grid(self._h, dir.encode()))
+
+    def write_radial_trace(self, dir: str, run: int = 0) -> None:
+        """WRITE_RADIAL_TRACE (output.f90:309-343): appends column (1, 1) of every zone."""
+        _lib.check(self.lib.solar_gpu_write_radial_trace(self._h, run, dir.encode()))
+
+    def output_plane(self) -> int:
+        k = ctypes.c_int()
+        _lib.check(self.lib.solar_gpu_output_plane(self._h, ctypes.byref(k)))
+        return k.value
+
     # ------------------------------------------------------------------ adjoint
     def set_receivers(self, loc) -> None:
         """Receivers as rows (zone 0..5, i, j, k) of fractional 0-based grid indices."""
