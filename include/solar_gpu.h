@@ -156,6 +156,27 @@ int solar_gpu_time_rk4(solar_ctx* c, int nsteps, int per_kernel, double* out7);
 /* Block until the context's stream is idle. */
 int solar_gpu_synchronize(solar_ctx* c);
 
+/* ---- Source term of the v_r equation (nruns == 1) ------------------------------------
+ * SOLAR_FORCING_ANALYTIC: compute_rhs_acoustic.f90:92-104, S = mag(t) exp(-((theta-pi/2)/
+ *   (20 dxi))^2 - (phi/(20 dxi))^2 - ((r-r_c)/(20 dchi))^2) with mag(t) = exp(-(tau-650)^2/
+ *   (2*200^2)) cos(4 pi (tau-650)/700), tau = t rsun/c(row 1).  r_c = r of plane k_center
+ *   (0-based; the reference hard-codes gr(200), i.e. k_center = 199).
+ * SOLAR_FORCING_SAMPLES: the sampled source S_t(x,y,n) (READ_FORCING_FUNC, output.f90:271-
+ *   307) interpolated in time by LAGRANGE_INTERP (interpolation.f90:385-451) and added at
+ *   the plane e_rad (r nearest 1 - 100 km/R_sun), as the commented block of
+ *   compute_rhs_acoustic.f90:107-116 does; nstep is the run's step count (cube.f90:71),
+ *   which LAGRANGE_INTERP uses to drop its last two nodes.
+ * Every stage of one RK4 call uses the call's time; RK4 advances time by dt and the step
+ * counter by one (timestep.f90:82).  The clock starts at time 0, step 0. */
+#define SOLAR_FORCING_OFF 0
+#define SOLAR_FORCING_ANALYTIC 1
+#define SOLAR_FORCING_SAMPLES 2
+int solar_gpu_set_forcing(solar_ctx* c, int kind, int k_center, int nstep);
+/* Samples of one zone in the file order of READ_FORCING_FUNC: f[(i*ny + j)*nt + n]. */
+int solar_gpu_set_forcing_samples(solar_ctx* c, int zone, const double* f, int nt);
+int solar_gpu_set_clock(solar_ctx* c, double time, int step);
+int solar_gpu_get_clock(solar_ctx* c, double* time, int* step);
+
 /* ---- Zones split across processes (one GPU per process, nruns == 1) ---------------
  * The reference runs one MPI rank per zone block and exchanges interpolated halo strips
  * inside every derivative (derivative.f90:8-323).  Here a context can own a contiguous

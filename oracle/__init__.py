@@ -55,6 +55,12 @@ def _load():
     lib.oracle_rk4.argtypes = [ctypes.c_void_p, _D, ctypes.c_int]
     lib.oracle_norm.argtypes = [ctypes.c_void_p, _D, ctypes.c_int]
     lib.oracle_norm.restype = ctypes.c_double
+    lib.oracle_set_forcing.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.oracle_set_forcing.restype = ctypes.c_int
+    lib.oracle_set_forcing_samples.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, ctypes.c_int]
+    lib.oracle_set_forcing_samples.restype = ctypes.c_int
+    lib.oracle_set_clock.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
+    lib.oracle_get_clock.argtypes = [ctypes.c_void_p, _D, ctypes.POINTER(ctypes.c_int)]
     _lib = lib
     return lib
 
@@ -174,6 +180,24 @@ class Oracle:
         q = np.ascontiguousarray(q, dtype=np.float64).copy()
         self._lib.oracle_rk4(self._h, _p(q), int(nsteps))
         return q
+
+    # source term and clock (compute_rhs_acoustic.f90:92-116, timestep.f90:82)
+    def set_forcing(self, kind: int, k_center: int = 0, nstep: int = 0) -> None:
+        if self._lib.oracle_set_forcing(self._h, int(kind), int(k_center), int(nstep)) != 0:
+            raise ValueError("bad forcing arguments")
+
+    def set_forcing_samples(self, zone: int, f, nt: int) -> None:
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        if self._lib.oracle_set_forcing_samples(self._h, int(zone), _p(f), int(nt)) != 0:
+            raise ValueError("bad forcing samples")
+
+    def set_clock(self, time: float, step: int = 0) -> None:
+        self._lib.oracle_set_clock(self._h, float(time), int(step))
+
+    def get_clock(self):
+        t, s = ctypes.c_double(), ctypes.c_int()
+        self._lib.oracle_get_clock(self._h, ctypes.byref(t), ctypes.byref(s))
+        return t.value, s.value
 
     def norm(self, q, field: int = 4) -> float:
         q = np.ascontiguousarray(q, dtype=np.float64)

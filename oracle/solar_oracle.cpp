@@ -103,6 +103,16 @@ struct oracle_ctx {
   // 0: reference arithmetic.  1: on the eight strips that the receiver reverses,
   // evaluate the receiver-frame metric at the receiver's (mirrored) edge index.
   int fix_reversed_rotation = 0;
+  // source term of the v_r equation (compute_rhs_acoustic.f90:92-116): 0 off, 1 analytic
+  // (centre plane f_kcenter instead of the hard-coded gr(200)), 2 sampled S_t at e_rad
+  int forcing = 0, f_kcenter = 0, f_nstep = 0, f_nt = 0, e_rad = 0;
+  std::vector<double> f_samples;                      // S_t [zone][n][j][i]
+  // COMMON /TSTEP/ time, the driver's step, and LAGRANGE_INTERP's saved state
+  // (/STEP_TRACK/, /TIME_INTERP/, /LAGRANGE_TIME_INTERP/); advanced by RK4
+  mutable double time = 0.0;
+  mutable int step = 0, step_old = 0, f_error = 0;
+  mutable double xn[7] = {0, 0, 0, 0, 0, 0, 0};
+  mutable std::vector<double> LC;                     // [7][zone][j][i]
 };
 
 namespace {
@@ -614,8 +624,65 @@ void divergence_all(const oracle_ctx& c, const double* axi, const double* aeta, 
         }
 }
 
-// compute_rhs_acoustic.f90:1-159 COMPUTE_RHS, forcing magnitude 0 (term :92-104 and its
-// file output :119-125 are off).
+// interpolation.f90:385-451  LAGRANGE_INTERP: 7-point Lagrange interpolation in time of the
+// sampled source S_t; the nodes and coefficients are refreshed only when floor(xt) advances,
+// and the interpolant is evaluated at (step-1)*deltat.  Returns forcing [zone][j][i].
+void lagrange_interp(const oracle_ctx& c, std::vector<double>& forcing) {
+  const size_t P = c.plane, n6 = 6 * P;
+  const double cadforcing = 60.0 * c.dimc / c.diml;   // ic_acoustic_wave.f90:113
+  double xt = double(c.step) * c.dt / cadforcing + 1.0;
+  const int fl = (int)std::floor(xt);
+  if (c.LC.size() != 7 * n6) c.LC.assign(7 * n6, 0.0);
+  if (c.step_old < fl) {
+    double* x = c.xn;
+    x[0] = (xt - 4.0) * cadforcing;
+    x[1] = (xt - 3.0) * cadforcing;
+    x[2] = (xt - 2.0) * cadforcing;
+    x[3] = (xt - 1.0) * cadforcing;
+    x[4] = (xt)*cadforcing;
+    x[5] = (xt + 1.0) * cadforcing;
+    x[6] = (xt + 2.0) * cadforcing;
+    std::fill(c.LC.begin(), c.LC.end(), 0.0);
+    for (int m = 0; m < 7; ++m) {
+      bool on;
+      if (m <= 3) on = x[m] >= 0;
+      else if (m == 4) on = true;
+      else if (m == 5) on = fl < c.f_nstep;
+      else on = fl < c.f_nstep - 1;
+      if (!on) continue;
+      const int smp = fl - 3 + m;                    // S_t(:,:,floor(xt)-3+m), 1-based
+      if (smp < 1 || smp > c.f_nt) { c.f_error = 1; continue; }
+      double den = 0.0;
+      bool first = true;
+      for (int j = 0; j < 7; ++j) {
+        if (j == m) continue;
+        den = first ? (x[m] - x[j]) : den * (x[m] - x[j]);
+        first = false;
+      }
+      for (int z = 0; z < 6; ++z)
+        for (size_t p = 0; p < P; ++p)
+          c.LC[(size_t)m * n6 + z * P + p] = c.f_samples[((size_t)z * c.f_nt + (smp - 1)) * P + p] / den;
+    }
+    c.step_old = fl;
+  }
+  xt = (double(c.step) - 1.0) * c.dt;
+  const double* x = c.xn;
+  forcing.assign(n6, 0.0);
+  for (size_t p = 0; p < n6; ++p) {
+    double f = 0.0;
+    for (int m = 0; m < 7; ++m) {
+      double t = c.LC[(size_t)m * n6 + p];
+      for (int j = 0; j < 7; ++j)
+        if (j != m) t = t * (xt - x[j]);
+      f = (m == 0) ? t : f + t;
+    }
+    forcing[p] = f;
+  }
+}
+
+// compute_rhs_acoustic.f90:1-159 COMPUTE_RHS.  The source term :92-104 (analytic) or the
+// commented sampled form :107-116 is added when the context enables it; the forcing_rms
+// file output :119-125 is not reproduced.
 void compute_rhs_all(const oracle_ctx& c, const double* q, double* rhs) {
   const size_t V = c.vol;
   auto Q = [&](int z, int m) { return q + ((size_t)z * 5 + m) * V; };
@@ -651,6 +718,27 @@ void compute_rhs_all(const oracle_ctx& c, const double* q, double* rhs) {
           R(z, 4)[l] = r5;
         }
     }
+  if (c.forcing == 1) {
+    const double u = c.time * c.diml / c.dimc - 650.0;
+    const double mag = std::exp(-(u * u) / (2.0 * 200.0 * 200.0)) * std::cos(4.0 * PI * u / 700.0);
+    const double w = 20.0 * c.dxi, wr = 20.0 * c.dchi;
+    for (int z = 0; z < 6; ++z)
+      for (int k = 0; k < c.nr; ++k)
+        for (int j = 0; j < n; ++j)
+          for (int i = 0; i < n; ++i) {
+            const size_t p = (size_t)z * c.plane + (size_t)j * n + i;
+            const double a = (c.theta[p] - PI / 2.0) / w, b = (c.phi[p] - 0.0) / w;
+            const double cc = (c.gr[k] - c.gr[c.f_kcenter]) / wr;
+            R(z, 3)[idx3(c, k, j, i)] += mag * std::exp(-(a * a) - b * b - cc * cc);
+          }
+  } else if (c.forcing == 2) {
+    std::vector<double> f;
+    lagrange_interp(c, f);
+    for (int z = 0; z < 6; ++z)
+      for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i)
+          R(z, 3)[idx3(c, c.e_rad, j, i)] += f[(size_t)z * c.plane + (size_t)j * n + i];
+  }
 }
 
 // bc_acoustic_wave.f90:1-36  BC_RHS: zero RHS at global k = 1 and k = nr
@@ -863,7 +951,52 @@ void oracle_rk4(const oracle_ctx* c, double* q, int nsteps) {
     }
     filter_exp_all(*c, q, qf.data());
     std::memcpy(q, qf.data(), N * sizeof(double));
+    c->time = c->time + c->dt;                         // timestep.f90:82
+    c->step = c->step + 1;                             // cube.f90:71 loop counter
   }
+}
+
+// Source term selection and its data (see oracle_ctx).
+int oracle_set_forcing(oracle_ctx* c, int kind, int k_center, int nstep) {
+  if (kind < 0 || kind > 2 || (kind == 1 && (k_center < 0 || k_center >= c->nr))) return -1;
+  if (kind == 2 && c->f_samples.empty()) return -1;
+  c->forcing = kind;
+  c->f_kcenter = k_center;
+  c->f_nstep = nstep;
+  // e_rad: plane nearest 1 - 100 km / R_sun (ic_acoustic_wave.f90:111, 117-122)
+  const double excitdep = 1.0 - 100e5 / c->diml;
+  double temp = 1.0;
+  for (int k = 0; k < c->nr; ++k)
+    if (std::fabs(c->gr[k] - excitdep) <= temp) {
+      temp = std::fabs(c->gr[k] - excitdep);
+      c->e_rad = k;
+    }
+  return 0;
+}
+
+// READ_FORCING_FUNC (output.f90:271-307): f(i, j, n) stored with n fastest, then j, then i.
+int oracle_set_forcing_samples(oracle_ctx* c, int zone, const double* f, int nt) {
+  if (zone < 0 || zone > 5 || nt < 1 || (c->f_nt && nt != c->f_nt)) return -1;
+  const int n = c->nx;
+  if (c->f_samples.empty()) { c->f_samples.assign((size_t)6 * nt * c->plane, 0.0); c->f_nt = nt; }
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j)
+      for (int m = 0; m < nt; ++m)
+        c->f_samples[((size_t)zone * nt + m) * c->plane + (size_t)j * n + i] = f[((size_t)i * n + j) * nt + m];
+  return 0;
+}
+
+void oracle_set_clock(oracle_ctx* c, double time, int step) {
+  c->time = time;
+  c->step = step;
+  c->step_old = 0;
+  for (double& v : c->xn) v = 0.0;
+  c->LC.clear();
+}
+
+void oracle_get_clock(const oracle_ctx* c, double* time, int* step) {
+  if (time) *time = c->time;
+  if (step) *step = c->step;
 }
 
 // auxiliary.f90:100-125  norm: (sum/(nx*ny*nr)*6)**0.5 over all zones (the reference

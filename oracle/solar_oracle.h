@@ -79,6 +79,15 @@ void oracle_filter_exp(const oracle_ctx* c, const double* q, double* qf);
 void oracle_rk4(const oracle_ctx* c, double* q, int nsteps);
 double oracle_norm(const oracle_ctx* c, const double* q, int field);
 
+/* Source term of the v_r equation (compute_rhs_acoustic.f90:92-116): kind 0 off, 1 analytic
+ * with centre plane k_center (0-based), 2 sampled S_t (LAGRANGE_INTERP) at plane e_rad;
+ * nstep = the run's step count.  Samples in READ_FORCING_FUNC order f[(i*nx + j)*nt + n].
+ * The clock (time, step) starts at 0 and RK4 advances it. */
+int oracle_set_forcing(oracle_ctx* c, int kind, int k_center, int nstep);
+int oracle_set_forcing_samples(oracle_ctx* c, int zone, const double* f, int nt);
+void oracle_set_clock(oracle_ctx* c, double time, int step);
+void oracle_get_clock(const oracle_ctx* c, double* time, int* step);
+
 #ifdef __cplusplus
 }
 #endif

@@ -20,6 +20,9 @@ SOLAR_ERR_NAN = -3
 SOLAR_ERR_TIMEOUT = -4
 SOLAR_ERR_STATE = -5
 SOLAR_ERR_NOMEM = -6
+SOLAR_FORCING_OFF = 0
+SOLAR_FORCING_ANALYTIC = 1
+SOLAR_FORCING_SAMPLES = 2
 SOLAR_FP64 = 0
 SOLAR_FP32 = 1
 
@@ -84,6 +87,10 @@ EXPORTS = {
     "solar_gpu_unpack_lines": [_P, ctypes.c_int, _I, ctypes.c_int, ctypes.c_void_p],
     "solar_gpu_stream": [_P],
     "solar_gpu_reduce_owned": [_P, ctypes.c_int, ctypes.c_int, _D],
+    "solar_gpu_set_forcing": [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int],
+    "solar_gpu_set_forcing_samples": [_P, ctypes.c_int, _D, ctypes.c_int],
+    "solar_gpu_set_clock": [_P, ctypes.c_double, ctypes.c_int],
+    "solar_gpu_get_clock": [_P, _D, _I],
     "solar_gpu_write_restart": [_P, ctypes.c_int, ctypes.c_char_p, ctypes.c_int, ctypes.c_double, ctypes.c_int],
     "solar_gpu_read_restart": [_P, ctypes.c_int, ctypes.c_char_p, ctypes.c_int, _D, _I],
     "solar_gpu_write_visual": [_P, ctypes.c_int, ctypes.c_char_p, ctypes.c_int],

@@ -140,6 +140,7 @@ static int enqueue_step_div(solar_ctx* c, T* dstep) {
   void* bufs[2] = {c->A, c->B};
   const long long V6 = 6 * vol_compact(c);
   int cur = 0, rc;
+  if ((rc = force_begin(c))) return rc;
   for (int s = 0; s < 5; ++s) {
     if ((rc = launch_edge<T>(c, bufs[cur], 0, nullptr))) return rc;
     if ((rc = launch_stage<T>(c, bufs[cur], bufs[cur ^ 1], s == 0 ? 4 : 5, s, nullptr, dstep + s * V6))) return rc;
@@ -148,7 +149,7 @@ static int enqueue_step_div(solar_ctx* c, T* dstep) {
   if ((rc = launch_edge<T>(c, bufs[cur], 1, nullptr))) return rc;
   if ((rc = launch_filter<T>(c, bufs[cur], bufs[cur ^ 1], nullptr))) return rc;
   CK(cudaGetLastError());
-  return SOLAR_OK;
+  return force_end(c);
 }
 
 template <typename T>
@@ -168,6 +169,10 @@ static int misfit_gradient_t(solar_ctx* c, int N, int K, const double* data, dou
   if ((rc = adj_reserve(&b.ckpt, &b.ckpt_bytes, S * (size_t)ncp))) return rc;
   if ((rc = adj_reserve(&b.div, &b.div_bytes, (size_t)std::min(K, N) * 5 * V6 * sizeof(T)))) return rc;
   if ((rc = adj_reserve((void**)&b.traces, &b.traces_bytes, (size_t)std::max(N, 1) * b.nrec * 2 * sizeof(double)))) return rc;
+  // with a source term the clock (time, step, interpolation state) is checkpointed too
+  const size_t CL = sizeof(ForceClock);
+  if (c->forcing && (rc = adj_reserve(&b.clk, &b.clk_bytes, CL * (size_t)ncp))) return rc;
+  char* clk = (char*)b.clk;
   double* traces = b.traces;
   double* res = b.traces + (size_t)N * b.nrec;
   char* ckpt = (char*)b.ckpt;
@@ -176,7 +181,10 @@ static int misfit_gradient_t(solar_ctx* c, int N, int K, const double* data, dou
   CK(cudaEventRecord(c->ev[2], c->stream));
   // forward sweep: checkpoints every K steps, receiver traces after every step
   for (int n = 0; n < N; ++n) {
-    if (n % K == 0) CK(cudaMemcpyAsync(ckpt + (size_t)(n / K) * S, c->A, S, cudaMemcpyDeviceToDevice, c->stream));
+    if (n % K == 0) {
+      CK(cudaMemcpyAsync(ckpt + (size_t)(n / K) * S, c->A, S, cudaMemcpyDeviceToDevice, c->stream));
+      if (c->forcing) CK(cudaMemcpyAsync(clk + (size_t)(n / K) * CL, c->force_clock, CL, cudaMemcpyDeviceToDevice, c->stream));
+    }
     CK(cudaGraphLaunch(c->step_graph, c->stream));
     enqueue_sample<T>(c, traces + (size_t)n * b.nrec);
   }
@@ -200,6 +208,7 @@ static int misfit_gradient_t(solar_ctx* c, int N, int K, const double* data, dou
     const int n0 = seg * K, n1 = std::min(N, n0 + K);
     CK(cudaEventRecord(c->ev[4], c->stream));
     CK(cudaMemcpyAsync(c->A, ckpt + (size_t)seg * S, S, cudaMemcpyDeviceToDevice, c->stream));
+    if (c->forcing) CK(cudaMemcpyAsync(c->force_clock, clk + (size_t)seg * CL, CL, cudaMemcpyDeviceToDevice, c->stream));
     for (int n = n0; n < n1; ++n)
       if ((rc = enqueue_step_div<T>(c, D + (size_t)(n - n0) * 5 * V6))) return rc;
     CK(cudaEventRecord(c->ev[5], c->stream));
@@ -217,8 +226,9 @@ static int misfit_gradient_t(solar_ctx* c, int N, int K, const double* data, dou
     t_rec += r;
     t_adj += a;
   }
-  // leave the state at the initial condition
+  // leave the state (and the clock) at the initial condition
   CK(cudaMemcpyAsync(c->A, ckpt, S, cudaMemcpyDeviceToDevice, c->stream));
+  if (c->forcing) CK(cudaMemcpyAsync(c->force_clock, clk, CL, cudaMemcpyDeviceToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   if ((rc = check_device_error(c))) return rc;
   if (times) {

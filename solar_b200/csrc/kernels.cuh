@@ -322,6 +322,8 @@ struct StageArgs {
   const T* met;             // [kNumMetric][n][n]
   const T* c2;              // optional compact c^2 [face][k][j][i] (run-shared) or nullptr
   T* divout;                // MODE 4/5: compact divergence [face][k][j][i]
+  const T* force;           // FORCE: this step's forcing field [face][j][i] (v_r equation)
+  const T* force_r;         // FORCE: its radial factor [nr]
   const int* active;
   int* err;
   Geom g;
@@ -346,7 +348,7 @@ struct StageLayout {
 
 // Each thread owns V consecutive points of one row (V = 16 bytes / sizeof(T)), so the
 // CTA has (TX/V) x TY threads and every shared-memory access is a 16-byte vector.
-template <typename T, int TX, int TY, int MODE_, bool HAS_RHO>
+template <typename T, int TX, int TY, int MODE_, bool HAS_RHO, bool FORCE = false>
 __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __grid_constant__ StageArgs<T> a) {
   constexpr bool STORE_DIV = MODE_ >= 4;
   constexpr int MODE = MODE_ == 4 ? 1 : (MODE_ == 5 ? 0 : MODE_);
@@ -431,6 +433,8 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __
   ldv(a.met + mTX * P2 + p2, m_TX);
   ldv(a.met + mTY * P2 + p2, m_TY);
   const T c1 = Coef<T>::drp(1), c2 = Coef<T>::drp(2), c3 = Coef<T>::drp(3);
+  T f_xy[V];
+  if (FORCE) ldv(a.force + (long long)face * P2 + p2, f_xy);
   const long long own = g.at(0, j, ib);
   T* outS[5];
   T* qwS[5];
@@ -447,9 +451,10 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __
 
   // radial coefficients of the current plane; the next plane's are loaded one iteration
   // ahead so their latency hides behind the compute
-  struct Rad { T facr, invr, rho0, inv_rho0, c2rho0, rho0g0, sig, drho0, g0rho0; };
+  struct Rad { T facr, invr, rho0, inv_rho0, c2rho0, rho0g0, sig, drho0, g0rho0, frc; };
   auto load_rad = [&](int k) {
     Rad r;
+    r.frc = FORCE ? __ldg(a.force_r + k) : T(0);
     r.facr = __ldg(a.rad + rFacR * nr + k);
     r.invr = __ldg(a.rad + rInvR * nr + k);
     r.rho0 = __ldg(a.rad + rRho0 * nr + k);
@@ -564,6 +569,7 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __
           r_rho[q] = -rho0 * div - v_r * rc.drho0;
           r_vr[q] -= rho[q] * rc.g0rho0;
         }
+        if (FORCE) r_vr[q] += f_xy[q] * rc.frc;         // + S(theta, phi, t) e_r
       }
     }
     const long long kp = (long long)k * g.plane;

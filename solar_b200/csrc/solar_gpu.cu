@@ -68,6 +68,8 @@ struct AdjBuffers {
   size_t ckpt_bytes = 0;
   void* div = nullptr;      // stage-input divergences of one checkpoint segment
   size_t div_bytes = 0;
+  void* clk = nullptr;      // source-term clocks of the checkpoints
+  size_t clk_bytes = 0;
   double* traces = nullptr; // receiver traces and residuals
   size_t traces_bytes = 0;
   long long* rec_off = nullptr;
@@ -103,6 +105,14 @@ struct solar_ctx {
   cudaGraphExec_t batch_graph = nullptr;
   cudaEvent_t ev[8] = {};
   AdjBuffers adj;
+  int forcing = 0;             // SOLAR_FORCING_*
+  int force_nstep = 0, force_nt = 0;
+  double force_cad = 0;        // forcing sample cadence, cadforcing (ic_acoustic_wave.f90:113)
+  void* force_clock = nullptr;  // ForceClock (device)
+  double* force_exy = nullptr;  // analytic: exp(-A^2 - B^2) [face][j][i]
+  double* force_samples = nullptr;  // sampled: S_t [nt][face][j][i]
+  void* force_xy = nullptr;     // this step's forcing field (kernel precision)
+  void* force_r = nullptr;      // radial factor (kernel precision)
   int* split_items = nullptr;  // (zone, edge) pairs of one line pack/unpack
   int* split_slots = nullptr;  // slots exchanged per phase
 };
@@ -227,7 +237,7 @@ static int launch_edge(solar_ctx* c, void* buf, int mode, const int* active) {
   }
 }
 
-template <typename T, int TX, int TY, int MODE, bool HAS_RHO>
+template <typename T, int TX, int TY, int MODE, bool HAS_RHO, bool FORCE = false>
 static int launch_stage_t(solar_ctx* c, StageArgs<T>& a, const void* qin) {
   using L = StageLayout<T, TX, TY, HAS_RHO>;
   if (!make_map(c, qin, TX + 8, TY + 6, &a.mP) || !make_map(c, qin, TX + 8, TY, &a.mX) ||
@@ -236,19 +246,29 @@ static int launch_stage_t(solar_ctx* c, StageArgs<T>& a, const void* qin) {
     return fail(SOLAR_ERR_CUDA, "cuTensorMapEncodeTiled failed");
   static bool attr_set = false;
   if (!attr_set) {
-    CK(cudaFuncSetAttribute(stage_kernel<T, TX, TY, MODE, HAS_RHO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    CK(cudaFuncSetAttribute(stage_kernel<T, TX, TY, MODE, HAS_RHO, FORCE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)L::TOTAL));
     attr_set = true;
   }
   const int nchunks = (c->g.nr + a.kchunk - 1) / a.kchunk;
   dim3 grid((c->g.n / TX) * (c->g.n / TY), nchunks, c->g.nruns * c->g.nface);
-  stage_kernel<T, TX, TY, MODE, HAS_RHO><<<grid, dim3(TX / Vec16<T>::V, TY), L::TOTAL, c->stream>>>(a);
+  stage_kernel<T, TX, TY, MODE, HAS_RHO, FORCE><<<grid, dim3(TX / Vec16<T>::V, TY), L::TOTAL, c->stream>>>(a);
   return SOLAR_OK;
 }
 
 template <typename T, int TX, int TY>
 static int launch_stage_mode(solar_ctx* c, StageArgs<T>& a, const void* qin, int mode) {
   const bool rho = c->g.slot[kRho] >= 0;
+  if (a.force) {                    // forcing term (stepping and COMPUTE_RHS modes only)
+    switch (mode) {
+      case 0: return rho ? launch_stage_t<T, TX, TY, 0, true, true>(c, a, qin) : launch_stage_t<T, TX, TY, 0, false, true>(c, a, qin);
+      case 1: return rho ? launch_stage_t<T, TX, TY, 1, true, true>(c, a, qin) : launch_stage_t<T, TX, TY, 1, false, true>(c, a, qin);
+      case 2: return rho ? launch_stage_t<T, TX, TY, 2, true, true>(c, a, qin) : launch_stage_t<T, TX, TY, 2, false, true>(c, a, qin);
+      case 4: return rho ? launch_stage_t<T, TX, TY, 4, true, true>(c, a, qin) : launch_stage_t<T, TX, TY, 4, false, true>(c, a, qin);
+      case 5: return rho ? launch_stage_t<T, TX, TY, 5, true, true>(c, a, qin) : launch_stage_t<T, TX, TY, 5, false, true>(c, a, qin);
+      default: return fail(SOLAR_ERR_ARG, "forcing is not available in stage mode %d", mode);
+    }
+  }
   switch (mode) {
     case 0: return rho ? launch_stage_t<T, TX, TY, 0, true>(c, a, qin) : launch_stage_t<T, TX, TY, 0, false>(c, a, qin);
     case 1: return rho ? launch_stage_t<T, TX, TY, 1, true>(c, a, qin) : launch_stage_t<T, TX, TY, 1, false>(c, a, qin);
@@ -272,6 +292,9 @@ static int launch_stage(solar_ctx* c, const void* qin, void* qout, int mode, int
                         const int* active, void* divout = nullptr) {
   StageArgs<T> a;
   a.divout = (T*)divout;
+  const bool forced = c->forcing && mode != 3;     // every mode but the gradient/divergence operator
+  a.force = forced ? (const T*)c->force_xy : nullptr;
+  a.force_r = forced ? (const T*)c->force_r : nullptr;
   a.qout = (T*)qout;
   a.qw = (T*)c->W;
   a.rad = (const T*)c->dt.rad;
@@ -319,12 +342,16 @@ static int launch_filter(solar_ctx* c, const void* qin, void* qout, const int* a
   return launch_filter_t<T, 16, 16>(c, qin, qout, active);
 }
 
+static int force_begin(solar_ctx* c);   // forcing.cuh: this step's source field
+static int force_end(solar_ctx* c);     // forcing.cuh: time += dt, step += 1
+
 // One full time step (timestep.f90:61-82) on every run.  With ev != nullptr each kernel
 // is bracketed by events: ev_pairs[kind] accumulates into times[kind].
 template <typename T>
 static int enqueue_step(solar_ctx* c, const int* active, std::vector<cudaEvent_t>* evs) {
   void* bufs[2] = {c->A, c->B};
   int cur = 0, rc;
+  if ((rc = force_begin(c))) return rc;
   auto mark = [&]() {
     if (!evs) return;
     cudaEvent_t e;
@@ -345,7 +372,7 @@ static int enqueue_step(solar_ctx* c, const int* active, std::vector<cudaEvent_t
   mark();
   if ((rc = launch_filter<T>(c, bufs[cur], bufs[cur ^ 1], active))) return rc;
   mark();
-  return SOLAR_OK;
+  return force_end(c);
 }
 
 static int enqueue_step_any(solar_ctx* c, const int* active, std::vector<cudaEvent_t>* evs) {
@@ -359,6 +386,7 @@ static int check_device_error(solar_ctx* c) {
   CK(cudaStreamSynchronize(c->stream));
   if (h) {
     cudaMemsetAsync(c->err, 0, sizeof(int), c->stream);
+    if (h == 2) return fail(SOLAR_ERR_ARG, "forcing: a time sample outside the loaded samples was needed");
     return fail(SOLAR_ERR_TIMEOUT, "a device wait gave up (code %d)", h);
   }
   return SOLAR_OK;
@@ -516,7 +544,8 @@ int solar_gpu_finalize(solar_ctx* c) {
   for (void* p : ptrs)
     if (p) cudaFree(p);
   void* aptrs[] = {c->adj.L, c->adj.LW, c->adj.T1, c->adj.T2, c->adj.rb, c->adj.grad, c->adj.ckpt,
-                   c->adj.div, c->adj.traces, c->adj.rec_off, c->adj.rec_w, c->split_items, c->split_slots};
+                   c->adj.div, c->adj.traces, c->adj.rec_off, c->adj.rec_w, c->adj.clk, c->split_items, c->split_slots,
+                   c->force_clock, c->force_exy, c->force_samples, c->force_xy, c->force_r};
   for (void* p : aptrs)
     if (p) cudaFree(p);
   for (auto& e : c->ev)
@@ -717,6 +746,7 @@ int solar_gpu_compute_rhs(solar_ctx* c, const double* q, double* rhs) {
   if (rc) return rc;
   if (!q || !rhs) return fail(SOLAR_ERR_ARG, "null array");
   if ((rc = op_prepare_state(c, q))) return rc;
+  if ((rc = force_begin(c))) return rc;
   if (c->fp32) { launch_edge<float>(c, c->B, 0, nullptr); rc = launch_stage<float>(c, c->B, c->W, 2, 0, nullptr); }
   else { launch_edge<double>(c, c->B, 0, nullptr); rc = launch_stage<double>(c, c->B, c->W, 2, 0, nullptr); }
   if (rc) return rc;
@@ -882,6 +912,7 @@ int solar_gpu_synchronize(solar_ctx* c) {
 
 }  // extern "C"
 
-#include "adjoint_host.cuh"
 #include "split_host.cuh"
 #include "io_host.cuh"
+#include "forcing.cuh"
+#include "adjoint_host.cuh"

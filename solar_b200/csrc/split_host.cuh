@@ -58,6 +58,7 @@ static int lines_op(solar_ctx* c, int phase, const int* zone_edge, int count, vo
 template <typename T>
 static int enqueue_phase(solar_ctx* c, int phase) {
   int rc;
+  if (phase == 0 && (rc = force_begin(c))) return rc;
   if (phase < 5) {
     void* in = phase % 2 ? c->B : c->A;
     void* out = phase % 2 ? c->A : c->B;
@@ -65,7 +66,8 @@ static int enqueue_phase(solar_ctx* c, int phase) {
     return launch_stage<T>(c, in, out, phase == 0 ? 1 : 0, phase, nullptr);
   }
   if ((rc = launch_edge<T>(c, c->B, 1, nullptr))) return rc;
-  return launch_filter<T>(c, c->B, c->A, nullptr);
+  if ((rc = launch_filter<T>(c, c->B, c->A, nullptr))) return rc;
+  return force_end(c);
 }
 
 }  // namespace solar

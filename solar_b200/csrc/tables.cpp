@@ -74,6 +74,7 @@ int build_tables(const solar_desc& d, HostTables& t, std::string& err) {
   // SOLAR_DATA (ic_acoustic_wave.f90:236-271): normalise by the first row.
   const double* M = d.model;
   const double dimc = M[1], dimrho = M[2], diml = 695.9894e8;
+  t.dimc = dimc;
   if (dimc == 0.0 || dimrho == 0.0) { err = "model row 1 has zero c or rho"; return SOLAR_ERR_ARG; }
   t.gr.resize(nr); t.c2.resize(nr); t.rho0.resize(nr); t.g0.resize(nr);
   for (int k = 0; k < nr; ++k) {

@@ -63,6 +63,7 @@ enum Metric {
 struct HostTables {
   int n = 0, nr = 0;
   double dxi = 0, dchi = 0;
+  double dimc = 1;                                 // model row 1 sound speed (SOLAR_DATA's dimc)
   std::vector<double> gxi, gr, gdrdchi, tanx;     // 1-D grids (gxi == geta)
   std::vector<double> c2, rho0, g0;                // normalised radial background
   std::vector<double> radial;                      // [kNumRadial][nr]

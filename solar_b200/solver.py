@@ -203,6 +203,25 @@ class Solver:
     def synchronize(self) -> None:
         _lib.check(self.lib.solar_gpu_synchronize(self._h))
 
+    # ------------------------------------------------------------------ source term
+    def set_forcing(self, kind: int, k_center: int = 0, nstep: int = 0) -> None:
+        """v_r source of COMPUTE_RHS: 0 off, 1 analytic (compute_rhs_acoustic.f90:92-104,
+        centre plane k_center), 2 sampled S_t with LAGRANGE_INTERP at plane e_rad."""
+        _lib.check(self.lib.solar_gpu_set_forcing(self._h, int(kind), int(k_center), int(nstep)))
+
+    def set_forcing_samples(self, zone: int, f: np.ndarray, nt: int) -> None:
+        """Samples of one zone in READ_FORCING_FUNC order: f[(i*nx + j)*nt + n]."""
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        _lib.check(self.lib.solar_gpu_set_forcing_samples(self._h, int(zone), _ptr(f), int(nt)))
+
+    def set_clock(self, time: float, step: int = 0) -> None:
+        _lib.check(self.lib.solar_gpu_set_clock(self._h, float(time), int(step)))
+
+    def get_clock(self):
+        t, s = ctypes.c_double(), ctypes.c_int()
+        _lib.check(self.lib.solar_gpu_get_clock(self._h, ctypes.byref(t), ctypes.byref(s)))
+        return t.value, s.value
+
     # ------------------------------------------------------------------ output files
     def write_restart(self, dir: str, cue: int, time: float, step: int, run: int = 0) -> None:
         """WRITE_RESTART (output.f90:86-190) for the six zones of `run`."""
