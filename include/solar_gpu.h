@@ -110,7 +110,7 @@ int solar_gpu_rk4_runs(solar_ctx* c, const int* nsteps_per_run);
 int solar_gpu_time_rk4_runs(solar_ctx* c, const int* nsteps_per_run, double* ms);
 
 /* Operator-level drop-ins (host arrays in, host arrays out; use run 0's buffers):
- *   COMPUTE_RHS (compute_rhs_acoustic.f90:1-159, forcing off)        q -> rhs
+ *   COMPUTE_RHS (compute_rhs_acoustic.f90:1-159; source term as set) q -> rhs
  *   BC_RHS      (bc_acoustic_wave.f90:1-36)                          rhs in place
  *   SPONGE      (sponge.f90:1-58)                                    q, rhs in place
  *   FILTER_EXP  (filter.f90:9-48)                                    q -> qf
@@ -174,6 +174,9 @@ int solar_gpu_synchronize(solar_ctx* c);
 int solar_gpu_set_forcing(solar_ctx* c, int kind, int k_center, int nstep);
 /* Samples of one zone in the file order of READ_FORCING_FUNC: f[(i*ny + j)*nt + n]. */
 int solar_gpu_set_forcing_samples(solar_ctx* c, int zone, const double* f, int nt);
+/* READ_FORCING_FUNC (output.f90:271-307): the six files dir/forcing/forcing_cubesph.<z+1>,
+ * each one unformatted record of nx*nx*nt float64 values, into the sampled source. */
+int solar_gpu_load_forcing(solar_ctx* c, const char* dir, int nt);
 int solar_gpu_set_clock(solar_ctx* c, double time, int step);
 int solar_gpu_get_clock(solar_ctx* c, double* time, int* step);
 
@@ -247,6 +250,7 @@ int solar_io_read_restart(const char* path, double* q, int nx, int ny, int nr, d
 int solar_io_write_visual(const char* path, const double* plane5, int nx, int ny);
 int solar_io_write_grid(const char* path, const int* seven);
 int solar_io_append_trace(const char* path, const double* values, int count);
+int solar_io_read_forcing(const char* path, int nx, int ny, int nt, double* f);
 
 /* ---- Discrete adjoint (run 0 of a context with nruns == 1) -------------------------
  * No counterpart in the reference, which has no adjoint.  These are the exact transposes

@@ -89,6 +89,8 @@ EXPORTS = {
     "solar_gpu_reduce_owned": [_P, ctypes.c_int, ctypes.c_int, _D],
     "solar_gpu_set_forcing": [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int],
     "solar_gpu_set_forcing_samples": [_P, ctypes.c_int, _D, ctypes.c_int],
+    "solar_gpu_load_forcing": [_P, ctypes.c_char_p, ctypes.c_int],
+    "solar_io_read_forcing": [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _D],
     "solar_gpu_set_clock": [_P, ctypes.c_double, ctypes.c_int],
     "solar_gpu_get_clock": [_P, _D, _I],
     "solar_gpu_write_restart": [_P, ctypes.c_int, ctypes.c_char_p, ctypes.c_int, ctypes.c_double, ctypes.c_int],

@@ -10,6 +10,8 @@
 //   visual    output.f90:192-240  Fortran unformatted sequential record of q(:,:,o_rad,1:5)
 //                                 in 'Visual/NNN/vis_<rank>' (record markers: 4-byte lengths).
 //   grid      output.f90:242-267  'Visual/grid/grid_<rank>', FORMAT(1x, 7i5).
+//   forcing   output.f90:271-307  'forcing/forcing_cubesph.<zone>' (read only): one record of
+//                                 f(nx, ny, nt) with n fastest.
 //   trace     output.f90:309-343  'trace_<zone>', appended, ((q(1,1,k,l), k=1,mr), l=1,5)
 //                                 with FORMAT(1x, 5(ES13.5)): five values per line, the
 //                                 leading blank on the first line only (format reversion).
@@ -119,6 +121,26 @@ int solar_io_read_restart(const char* path, double* q, int nx, int ny, int nr, d
   if (!ok) return io_fail(std::string("short restart file ") + path);
   if (time) *time = t;
   if (step) *step = st;
+  return SOLAR_OK;
+}
+
+// READ_FORCING_FUNC (output.f90:271-307): 'forcing/forcing_cubesph.<zone>', one unformatted
+// sequential record of f(nx, ny, nt) written with n fastest, then j, then i.  `f` receives
+// the record as stored: f[(i*ny + j)*nt + n].
+int solar_io_read_forcing(const char* path, int nx, int ny, int nt, double* f) {
+  if (!path || !f || nx < 1 || ny < 1 || nt < 1) return io_fail("bad forcing arguments");
+  FILE* fp = std::fopen(path, "rb");
+  if (!fp) return io_fail(std::string("cannot open ") + path);
+  const size_t n = (size_t)nx * ny * nt;
+  int32_t head = 0, tail = 0;
+  bool ok = std::fread(&head, sizeof head, 1, fp) == 1 && (size_t)head == n * sizeof(double) &&
+            std::fread(f, sizeof(double), n, fp) == n && std::fread(&tail, sizeof tail, 1, fp) == 1 && tail == head;
+  std::fclose(fp);
+  if (!ok) {
+    char m[256];
+    std::snprintf(m, sizeof m, "%s is not one record of %d x %d x %d float64 values", path, nx, ny, nt);
+    return io_fail(m);
+  }
   return SOLAR_OK;
 }
 

@@ -10,6 +10,8 @@ int solar_io_read_restart(const char* path, double* q, int nx, int ny, int nr, d
 int solar_io_write_visual(const char* path, const double* plane5, int nx, int ny);
 int solar_io_write_grid(const char* path, const int* seven);
 int solar_io_append_trace(const char* path, const double* values, int count);
+int solar_io_read_forcing(const char* path, int nx, int ny, int nt, double* f);
+int solar_gpu_set_forcing_samples(solar_ctx* c, int zone, const double* f, int nt);
 }
 
 namespace solar {
@@ -129,6 +131,19 @@ int solar_gpu_write_radial_trace(solar_ctx* c, int run, const char* dir) {
   for (int z = 0; z < 6; ++z) {
     const std::string path = std::string(dir) + "/trace_" + std::to_string(z + 1);
     if ((rc = solar_io_append_trace(path.c_str(), h.data() + z * per, (int)per))) return rc;
+  }
+  return SOLAR_OK;
+}
+
+int solar_gpu_load_forcing(solar_ctx* c, const char* dir, int nt) {
+  int rc = check_out_args(c, 0, dir);
+  if (rc) return rc;
+  if (nt < 1) return fail(SOLAR_ERR_ARG, "nt < 1");
+  std::vector<double> f((size_t)c->g.n * c->g.n * nt);
+  for (int z = 0; z < 6; ++z) {
+    const std::string path = std::string(dir) + "/forcing/forcing_cubesph." + std::to_string(z + 1);
+    if ((rc = solar_io_read_forcing(path.c_str(), c->g.n, c->g.n, nt, f.data()))) return rc;
+    if ((rc = solar_gpu_set_forcing_samples(c, z, f.data(), nt))) return rc;
   }
   return SOLAR_OK;
 }

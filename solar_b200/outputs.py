@@ -79,3 +79,25 @@ def read_trace(path: str, nr: int) -> np.ndarray:
         body = line[1:] if len(line) % 13 == 1 else line
         vals += [parse_es(body[13 * q:13 * q + 13]) for q in range(len(body) // 13)]
     return np.array(vals).reshape(-1, 5, nr)
+
+
+def write_forcing(path: str, f: np.ndarray) -> None:
+    """A forcing_cubesph file: one unformatted record of f(nx, ny, nt) with n fastest;
+    ``f`` has shape (nx, ny, nt) indexed [i][j][n]."""
+    f = np.ascontiguousarray(f, dtype="<f8")
+    d = os.path.dirname(path)
+    if d:
+        os.makedirs(d, exist_ok=True)
+    with open(path, "wb") as fp:
+        marker = struct.pack("<i", f.nbytes)
+        fp.write(marker)
+        fp.write(f.tobytes())
+        fp.write(marker)
+
+
+def read_forcing(path: str, nx: int, ny: int, nt: int) -> np.ndarray:
+    """f[i][j][n] of a forcing_cubesph file."""
+    out = np.empty(nx * ny * nt)
+    _lib.check(_lib.load().solar_io_read_forcing(path.encode(), nx, ny, nt,
+                                                 out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+    return out.reshape(nx, ny, nt)

@@ -214,6 +214,10 @@ class Solver:
         f = np.ascontiguousarray(f, dtype=np.float64)
         _lib.check(self.lib.solar_gpu_set_forcing_samples(self._h, int(zone), _ptr(f), int(nt)))
 
+    def load_forcing(self, dir: str, nt: int) -> None:
+        """READ_FORCING_FUNC: dir/forcing/forcing_cubesph.<zone> for the six zones."""
+        _lib.check(self.lib.solar_gpu_load_forcing(self._h, dir.encode(), int(nt)))
+
     def set_clock(self, time: float, step: int = 0) -> None:
         _lib.check(self.lib.solar_gpu_set_clock(self._h, float(time), int(step)))
 

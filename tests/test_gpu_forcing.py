@@ -150,3 +150,20 @@ def test_adjoint_gradient_with_source(cfg):
     fd = (jp - jm) / (2 * eps)
     ad = float(np.vdot(res["grad_c"].ravel(), d.ravel()))
     assert abs(fd - ad) <= 1e-4 * abs(ad), (fd, ad)
+
+
+def test_forcing_files_load_like_set_samples(cfg, tmp_path):
+    from solar_b200 import outputs
+    nt = 24
+    S = samples(cfg, nt, 7)
+    for z in range(6):
+        outputs.write_forcing(str(tmp_path / "forcing" / f"forcing_cubesph.{z + 1}"), S[z].reshape(cfg.nx, cfg.nx, nt))
+    with Solver(cfg) as a, Solver(cfg) as b:
+        a.load_forcing(str(tmp_path), nt)
+        for z in range(6):
+            b.set_forcing_samples(z, S[z], nt)
+        for s in (a, b):
+            s.set_forcing(2, 0, 200)
+            s.set_state(np.zeros(s.state_shape))
+            s.rk4(12)
+        np.testing.assert_array_equal(a.get_state(), b.get_state())

@@ -91,3 +91,16 @@ def test_trace_records_append(tmp_path):
     assert got.shape == (2, 5, nr)
     for g, r in zip(got, recs):
         np.testing.assert_allclose(g.ravel(), r, rtol=6e-6, atol=1e-300)
+
+
+def test_forcing_file_roundtrip(tmp_path):
+    nx, nt = 5, 7
+    f = np.random.default_rng(2).standard_normal((nx, nx, nt))
+    path = str(tmp_path / "forcing" / "forcing_cubesph.3")
+    outputs.write_forcing(path, f)
+    raw = open(path, "rb").read()
+    assert len(raw) == f.size * 8 + 8
+    assert struct.unpack("<i", raw[:4])[0] == f.size * 8
+    np.testing.assert_array_equal(outputs.read_forcing(path, nx, nx, nt), f)
+    with pytest.raises(_lib.SolarError):
+        outputs.read_forcing(path, nx, nx, nt + 1)
