@@ -125,6 +125,13 @@ int solar_gpu_gradient(solar_ctx* c, const double* p, double* grad_xi, double* g
 int solar_gpu_divergence(solar_ctx* c, const double* v_xi, const double* v_eta,
                          const double* v_r, double* div);
 
+/* COMPUTE_CURL (grad.f90:140-255) with its halo transform TRANSFORM_VECTOR_BETWEEN_MESHES_CURL
+ * (transform.f90:279-498): (a_xi, a_eta, a_r) -> (curl_xi, curl_eta, curl_r), six-zone fields.
+ * Not used by the acoustics; the reference's defect on the eight reversed strips applies
+ * here too, and fix_reversed_rotation removes it. */
+int solar_gpu_curl(solar_ctx* c, const double* a_xi, const double* a_eta, const double* a_r, double* curl_xi,
+                   double* curl_eta, double* curl_r);
+
 /* norm (auxiliary.f90:100-125) of field m (1..5) of one run, in double:
  * (sum(f^2) / (nx*ny*nr) * 6)^0.5 over the six zones, the reference's formula. */
 int solar_gpu_norm(solar_ctx* c, int run, int field, double* out);

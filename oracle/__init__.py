@@ -55,6 +55,7 @@ def _load():
     lib.oracle_rk4.argtypes = [ctypes.c_void_p, _D, ctypes.c_int]
     lib.oracle_norm.argtypes = [ctypes.c_void_p, _D, ctypes.c_int]
     lib.oracle_norm.restype = ctypes.c_double
+    lib.oracle_curl.argtypes = [ctypes.c_void_p, _D, _D, _D, _D, _D, _D]
     lib.oracle_set_forcing.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     lib.oracle_set_forcing.restype = ctypes.c_int
     lib.oracle_set_forcing_samples.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, ctypes.c_int]
@@ -152,6 +153,13 @@ class Oracle:
         out = np.zeros_like(a[0])
         self._lib.oracle_divergence(self._h, _p(a[0]), _p(a[1]), _p(a[2]), _p(out))
         return out
+
+    def curl(self, axi, aeta, ar):
+        """COMPUTE_CURL (grad.f90:140-255): returns (curl_xi, curl_eta, curl_r)."""
+        a = [np.ascontiguousarray(x, dtype=np.float64) for x in (axi, aeta, ar)]
+        out = [np.zeros(self.field_shape) for _ in range(3)]
+        self._lib.oracle_curl(self._h, *(_p(x) for x in a), *(_p(x) for x in out))
+        return tuple(out)
 
     def filter_field(self, f, which: int):
         f = np.ascontiguousarray(f, dtype=np.float64)

@@ -564,6 +564,137 @@ void transform_div(const oracle_ctx& c, int z, const double* th, const double* p
       }
 }
 
+// transform.f90:279-498  TRANSFORM_VECTOR_BETWEEN_MESHES_CURL for zone z (1..6): both
+// receiver-frame components (xi, eta) of every strip this zone sends, from its interpolated
+// theta/phi strips.  Layout as transform_div: [edge][k][layer][t].
+void transform_curl(const oracle_ctx& c, int z, const double* th, const double* ph, double* oxi, double* oeta) {
+  const int n = c.nx;
+  const size_t ss = (size_t)c.nr * 3 * n;
+  double X[7], Y[7], C[7], D[7];  // index m+3, m = -3..3
+  for (int i = 1; i <= NST; ++i) {
+    X[3 - i] = std::tan(c.gxi[0] - i * c.dxi);
+    Y[3 - i] = std::tan(c.geta[0] - i * c.deta);
+    C[3 - i] = std::sqrt(1.0 + X[3 - i] * X[3 - i]);
+    D[3 - i] = std::sqrt(1.0 + Y[3 - i] * Y[3 - i]);
+    X[3 + i] = std::tan(c.gxi[n - 1] + i * c.dxi);
+    Y[3 + i] = std::tan(c.geta[n - 1] + i * c.deta);
+    C[3 + i] = std::sqrt(1.0 + X[3 + i] * X[3 + i]);
+    D[3 + i] = std::sqrt(1.0 + Y[3 + i] * Y[3 + i]);
+  }
+  std::vector<double> gC(n), gD(n);
+  for (int i = 0; i < n; ++i) {
+    gC[i] = std::pow(1.0 + std::pow(std::tan(c.gxi[i]), 2.0), 0.5);
+    gD[i] = std::pow(1.0 + std::pow(std::tan(c.geta[i]), 2.0), 0.5);
+  }
+  auto S = [&](const double* a, int e, int k, int m, int t) { return a[e * ss + ((size_t)k * 3 + (m - 1)) * n + t]; };
+  auto OX = [&](int e, int k, int m, int t) -> double& { return oxi[e * ss + ((size_t)k * 3 + (m - 1)) * n + t]; };
+  auto OE = [&](int e, int k, int m, int t) -> double& { return oeta[e * ss + ((size_t)k * 3 + (m - 1)) * n + t]; };
+  // the reversed strips (see transform_div): metric at the receiver's index when fixed
+  auto rev_strip = [&](int e) {
+    return (z == 2 && e == ES) || (z == 3 && (e == ES || e == EN)) || (z == 4 && e == EN) ||
+           (z == 5 && (e == EN || e == EW)) || (z == 6 && (e == ES || e == EE));
+  };
+  auto mt = [&](int e, int t) { return (c.fix_reversed_rotation && rev_strip(e)) ? n - 1 - t : t; };
+  for (int k = 0; k < c.nr; ++k)
+    for (int m = 1; m <= 3; ++m)
+      for (int t = 0; t < n; ++t) {
+        if (z <= 4) {  // transform.f90:314-332
+          for (int e : {EE, EW}) {
+            const int tj = mt(e, t);
+            const double Xm = (e == EE) ? X[3 - m] : X[3 + m], Cm = (e == EE) ? C[3 - m] : C[3 + m];
+            const double tg = std::tan(c.geta[tj]);
+            OX(e, k, m, t) = Cm * gD[tj] / std::sqrt(1.0 + Xm * Xm + tg * tg) * S(ph, e, k, m, t);
+            OE(e, k, m, t) = -S(th, e, k, m, t) + Xm * tg / std::sqrt(1.0 + Xm * Xm + tg * tg) * S(ph, e, k, m, t);
+          }
+        } else {        // transform.f90:339-390 (faces 5, 6 onto 1-4)
+          const double Ym = (z == 5) ? Y[3 + m] : Y[3 - m], Dm = (z == 5) ? D[3 + m] : D[3 - m];
+          for (int e : {ES, EN}) {
+            const int ti = mt(e, t);
+            const double tx = std::tan(c.gxi[ti]);
+            OE(e, k, m, t) = -S(th, e, k, m, t) + tx * Ym / std::sqrt(1.0 + tx * tx + Ym * Ym) * S(ph, e, k, m, t);
+            OX(e, k, m, t) = c.mC[ti] * Dm / std::sqrt(1.0 + tx * tx + Ym * Ym) * S(ph, e, k, m, t);
+          }
+          for (int e : {EE, EW}) {
+            const int ti = mt(e, t);
+            const double tx = std::tan(c.gxi[ti]);
+            OE(e, k, m, t) = -S(th, e, k, m, t) + tx * Ym / std::sqrt(1.0 + tx * tx + Ym * Ym) * S(ph, e, k, m, t);
+            OX(e, k, m, t) = gC[ti] * Dm / std::sqrt(1.0 + tx * tx + Ym * Ym) * S(ph, e, k, m, t);
+          }
+        }
+        // faces 1-4 onto face 5 (north, transform.f90:396-441) and face 6 (south, :446-493)
+        if (z <= 4) {
+          for (int e : {EN, ES}) {
+            const int ti = mt(e, t);
+            const double sg = (e == EN) ? 1.0 : -1.0;
+            const double thv = S(th, e, k, m, t), phv = S(ph, e, k, m, t);
+            if (z == 1 || z == 3) {
+              const bool plus = (z == 3) == (e == EN);     // z=1: N -> Y(-j), S -> Y(j); z=3 mirrored
+              const double Ym = plus ? Y[3 + m] : Y[3 - m], Dm = plus ? D[3 + m] : D[3 - m];
+              const double tx = std::tan(c.gxi[ti]);
+              const double s1 = std::sqrt(tx * tx + Ym * Ym), s2 = std::sqrt(1.0 + tx * tx + Ym * Ym);
+              OE(e, k, m, t) = sg * c.mC[ti] * Ym / s1 * thv + sg * c.mC[ti] / s1 * tx / s2 * phv;
+              OX(e, k, m, t) = sg * Dm * tx / s1 * thv - sg * Dm / s1 * Ym / s2 * phv;
+            } else {
+              const double Xm = (z == 2) ? X[3 + m] : X[3 - m], Cm = (z == 2) ? C[3 + m] : C[3 - m];
+              const double ty = std::tan(c.geta[ti]);
+              const double s1 = std::sqrt(Xm * Xm + ty * ty), s2 = std::sqrt(1.0 + Xm * Xm + ty * ty);
+              OX(e, k, m, t) = sg * gD[ti] * Xm / s1 * thv - sg * gD[ti] / s1 * ty / s2 * phv;
+              OE(e, k, m, t) = sg * Cm * ty / s1 * thv + sg * Cm / s1 * Xm / s2 * phv;
+            }
+          }
+        }
+      }
+}
+
+// grad.f90:140-255 COMPUTE_CURL over all zones
+void curl_all(const oracle_ctx& c, const double* axi, const double* aeta, const double* ar, double* cxi,
+              double* ceta, double* cr) {
+  const size_t ss = (size_t)c.nr * 3 * c.nx, V = c.vol;
+  std::vector<double> sr, hxr, hyr;
+  all_strips(c, ar, sr);
+  route_halos(c, sr, ROUTE_X, hxr);
+  route_halos(c, sr, ROUTE_Y, hyr);
+  std::vector<double> th(V), ph(V), sth(4 * ss), sph(4 * ss);
+  std::vector<double> sx((size_t)6 * 4 * ss, 0.0), se((size_t)6 * 4 * ss, 0.0);
+  for (int z = 0; z < 6; ++z) {
+    convert_xe_tp(c, z + 1, axi + z * V, aeta + z * V, th.data(), ph.data());
+    zone_strips(c, th.data(), sth.data());
+    zone_strips(c, ph.data(), sph.data());
+    transform_curl(c, z + 1, sth.data(), sph.data(), sx.data() + (size_t)z * 4 * ss, se.data() + (size_t)z * 4 * ss);
+  }
+  std::vector<double> hxx, hyx, hxe, hye;
+  route_halos(c, sx, ROUTE_X, hxx);
+  route_halos(c, sx, ROUTE_Y, hyx);
+  route_halos(c, se, ROUTE_X, hxe);
+  route_halos(c, se, ROUTE_Y, hye);
+  std::vector<double> d_r_xi(V), d_r_eta(V), d_xi_xi(V), d_eta_eta(V), d_eta_xi(V), d_xi_eta(V), d_xi_r(V), d_eta_r(V);
+  const int n = c.nx;
+  for (int z = 0; z < 6; ++z) {
+    auto hp = [&](const std::vector<double>& h, int side) { return h.data() + ((size_t)z * 2 + side) * ss; };
+    xi_stencil(c, ar + z * V, hp(hxr, 0), hp(hxr, 1), COEFFS1, 1.0 / c.dxi, d_r_xi.data());
+    eta_stencil(c, ar + z * V, hp(hyr, 0), hp(hyr, 1), COEFFS1, 1.0 / c.deta, d_r_eta.data());
+    xi_stencil(c, axi + z * V, hp(hxx, 0), hp(hxx, 1), COEFFS1, 1.0 / c.dxi, d_xi_xi.data());
+    eta_stencil(c, aeta + z * V, hp(hye, 0), hp(hye, 1), COEFFS1, 1.0 / c.deta, d_eta_eta.data());
+    xi_stencil(c, aeta + z * V, hp(hxe, 0), hp(hxe, 1), COEFFS1, 1.0 / c.dxi, d_eta_xi.data());
+    eta_stencil(c, axi + z * V, hp(hyx, 0), hp(hyx, 1), COEFFS1, 1.0 / c.deta, d_xi_eta.data());
+    ddr_zone(c, axi + z * V, d_xi_r.data());
+    ddr_zone(c, aeta + z * V, d_eta_r.data());
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < c.nr; ++k)
+      for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) {
+          const size_t p = (size_t)j * n + i, l = idx3(c, k, j, i), q = z * V + l;
+          const double sd = std::sqrt(c.delta[p]), XY = c.XY[p], CD = c.CD[p], rk = c.gr[k];
+          cxi[q] = XY / sd * d_xi_r[l] - CD / sd * d_eta_r[l] +
+                   (1.0 / rk) * (XY / sd * axi[q] - CD / sd * aeta[q] + sd / c.mD[j] * d_r_eta[l]);
+          ceta[q] = CD / sd * d_xi_r[l] - XY / sd * d_eta_r[l] +
+                    (1.0 / rk) * (CD / sd * axi[q] - XY / sd * aeta[q] - sd / c.mC[i] * d_r_xi[l]);
+          cr[q] = (sd / rk) * (XY / CD * (d_eta_eta[l] / c.mD[j] - d_xi_xi[l] / c.mC[i]) - d_xi_eta[l] / c.mD[j] +
+                               d_eta_xi[l] / c.mC[i]);
+        }
+  }
+}
+
 // ---------------------------------------------------------------- grad / div
 // grad.f90:13-59 COMPUTE_GRADIENT over all zones
 void gradient_all(const oracle_ctx& c, const double* a, double* gx, double* ge, double* gr) {
@@ -908,6 +1039,11 @@ void oracle_gradient(const oracle_ctx* c, const double* p, double* gxi, double* 
 void oracle_divergence(const oracle_ctx* c, const double* vxi, const double* veta, const double* vr,
                        double* div) {
   divergence_all(*c, vxi, veta, vr, div);
+}
+
+void oracle_curl(const oracle_ctx* c, const double* axi, const double* aeta, const double* ar, double* cxi,
+                 double* ceta, double* cr) {
+  curl_all(*c, axi, aeta, ar, cxi, ceta, cr);
 }
 
 void oracle_filter_field(const oracle_ctx* c, const double* f, double* out, int which) {

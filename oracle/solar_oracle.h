@@ -79,6 +79,11 @@ void oracle_filter_exp(const oracle_ctx* c, const double* q, double* qf);
 void oracle_rk4(const oracle_ctx* c, double* q, int nsteps);
 double oracle_norm(const oracle_ctx* c, const double* q, int field);
 
+/* COMPUTE_CURL (grad.f90:140-255) with TRANSFORM_VECTOR_BETWEEN_MESHES_CURL
+ * (transform.f90:279-498): (a_xi, a_eta, a_r) -> (curl_xi, curl_eta, curl_r), six-zone fields. */
+void oracle_curl(const oracle_ctx* c, const double* axi, const double* aeta, const double* ar, double* cxi,
+                 double* ceta, double* cr);
+
 /* Source term of the v_r equation (compute_rhs_acoustic.f90:92-116): kind 0 off, 1 analytic
  * with centre plane k_center (0-based), 2 sampled S_t (LAGRANGE_INTERP) at plane e_rad;
  * nstep = the run's step count.  Samples in READ_FORCING_FUNC order f[(i*nx + j)*nt + n].

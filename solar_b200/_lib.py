@@ -65,6 +65,7 @@ EXPORTS = {
     "solar_gpu_filter_exp": [_P, _D, _D],
     "solar_gpu_gradient": [_P, _D, _D, _D, _D],
     "solar_gpu_divergence": [_P, _D, _D, _D, _D],
+    "solar_gpu_curl": [_P, _D, _D, _D, _D, _D, _D],
     "solar_gpu_norm": [_P, ctypes.c_int, ctypes.c_int, _D],
     "solar_gpu_norm_noalloc": [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
     "solar_gpu_diag": [_P, ctypes.c_int, _D],

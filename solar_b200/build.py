@@ -19,7 +19,7 @@ LIB = os.path.join(HERE, "libsolar_gpu.so")
 SOURCES = [os.path.join(CSRC, "solar_gpu.cu"), os.path.join(CSRC, "noalloc.cu"), os.path.join(CSRC, "tables.cpp"),
            os.path.join(CSRC, "io.cpp")]
 HEADERS = [os.path.join(CSRC, h) for h in ("kernels.cuh", "tma.cuh", "tables.h", "adjoint.cuh", "adjoint_host.cuh",
-                                            "split_host.cuh", "io_host.cuh", "forcing.cuh")] + [os.path.join(ROOT, "include", "solar_gpu.h")]
+                                            "split_host.cuh", "io_host.cuh", "forcing.cuh", "curl.cuh")] + [os.path.join(ROOT, "include", "solar_gpu.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -47,6 +47,7 @@ struct DevTables {
   void* ew = nullptr;      // T [6][4][3][9][n]     folded edge weights (scalar)
   void* eg = nullptr;      // T [6][4][3][9][2][n]  folded edge weights (vector)
   int* s0t = nullptr;      // [6][4][3][n]          first tap of every ghost point
+  void* egc = nullptr;     // T [6][4][3][9][2][2][n] curl halo weights (both components), on first use
   void* c2 = nullptr;      // T [6][nr][n][n] optional
   double* rad64 = nullptr; // FP64 copies for diagnostics
   double* vol2 = nullptr;  // [n][n]
@@ -539,7 +540,7 @@ int solar_gpu_finalize(solar_ctx* c) {
   if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
   if (c->batch_graph) cudaGraphExecDestroy(c->batch_graph);
   void* ptrs[] = {c->A, c->B, c->W, c->stage64, c->part, c->red_out, c->active, c->target, c->done,
-                  c->err, c->dt.rad, c->dt.met, c->dt.ew, c->dt.eg, c->dt.s0t, c->dt.c2,
+                  c->err, c->dt.rad, c->dt.met, c->dt.ew, c->dt.eg, c->dt.egc, c->dt.s0t, c->dt.c2,
                   c->dt.rad64, c->dt.vol2, c->dt.drw, c->dt.c2_64, c->dt.tanx, c->dt.gr};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -916,3 +917,4 @@ int solar_gpu_synchronize(solar_ctx* c) {
 #include "io_host.cuh"
 #include "forcing.cuh"
 #include "adjoint_host.cuh"
+#include "curl.cuh"

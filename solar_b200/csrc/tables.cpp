@@ -261,10 +261,65 @@ int build_tables(const solar_desc& d, HostTables& t, std::string& err) {
       }
     }
 
+  // Both receiver-frame components of every vector strip, for COMPUTE_CURL
+  // (TRANSFORM_VECTOR_BETWEEN_MESHES_CURL, transform.f90:279-498), indexed like ROT:
+  // component out (0 xi, 1 eta) = cth * theta_interp + cph * phi_interp.
+  std::vector<double> rotc((size_t)6 * 4 * 3 * n * 4, 0.0);
+  auto RC = [&](int z, int e, int l, int q, int o, int c) -> double& {
+    return rotc[(((((size_t)z * 4 + e) * 3 + l) * n + q) * 2 + o) * 2 + c];
+  };
+  for (int z = 0; z < 6; ++z)
+    for (int e = 0; e < 4; ++e) {
+      const bool mirror = d.fix_reversed_rotation && reversed_on_receipt(z, e);
+      for (int l = 0; l < 3; ++l) {
+        const int m = l + 1;
+        for (int q = 0; q < n; ++q) {
+          const int qq = mirror ? n - 1 - q : q;
+          const double tq = t.tanx[qq], Cq = std::sqrt(1.0 + tq * tq);
+          double xt = 0, xp = 0, et = 0, ep = 0;          // (xi, eta) x (theta, phi)
+          if (z <= 3 && (e == kE || e == kW)) {           // transform.f90:314-332
+            const double X = (e == kE) ? Xm[m] : Xp[m], sx = std::sqrt(1.0 + X * X + tq * tq);
+            xp = std::sqrt(1.0 + X * X) * Cq / sx;
+            et = -1.0;
+            ep = X * tq / sx;
+          } else if (z >= 4) {                             // transform.f90:339-390
+            const double Y = (z == 4) ? Xp[m] : Xm[m], sy = std::sqrt(1.0 + tq * tq + Y * Y);
+            et = -1.0;
+            ep = tq * Y / sy;
+            xp = Cq * std::sqrt(1.0 + Y * Y) / sy;
+          } else {                                         // faces 1-4 onto 5 / 6 (:396-493)
+            const double sg = (e == kN) ? 1.0 : -1.0;
+            if (z == 0 || z == 2) {
+              const double Y = ((z == 2) == (e == kN)) ? Xp[m] : Xm[m];
+              const double s1 = std::sqrt(tq * tq + Y * Y), s2 = std::sqrt(1.0 + tq * tq + Y * Y);
+              const double Dy = std::sqrt(1.0 + Y * Y);
+              et = sg * Cq * Y / s1;
+              ep = sg * Cq / s1 * tq / s2;
+              xt = sg * Dy * tq / s1;
+              xp = -sg * Dy / s1 * Y / s2;
+            } else {
+              const double X = (z == 1) ? Xp[m] : Xm[m];
+              const double s1 = std::sqrt(X * X + tq * tq), s2 = std::sqrt(1.0 + X * X + tq * tq);
+              const double Cx = std::sqrt(1.0 + X * X);
+              xt = sg * Cq * X / s1;
+              xp = -sg * Cq / s1 * tq / s2;
+              et = sg * Cx * tq / s1;
+              ep = sg * Cx / s1 * X / s2;
+            }
+          }
+          RC(z, e, l, q, 0, 0) = xt;
+          RC(z, e, l, q, 0, 1) = xp;
+          RC(z, e, l, q, 1, 0) = et;
+          RC(z, e, l, q, 1, 1) = ep;
+        }
+      }
+    }
+
   // Fold everything an edge value needs into one set of coefficients per ghost point.
   t.ew.assign((size_t)6 * 4 * 3 * 9 * n, 0.0);
   t.eg.assign((size_t)6 * 4 * 3 * 9 * 2 * n, 0.0);
   t.s0t.assign((size_t)6 * 4 * 3 * n, 0);
+  t.egc.assign((size_t)6 * 4 * 3 * 9 * 4 * n, 0.0);
   for (int f = 0; f < 6; ++f)
     for (int e = 0; e < 4; ++e) {
       const EdgeRoute rt = kRoutes[f][e];
@@ -288,6 +343,11 @@ int build_tables(const solar_desc& d, HostTables& t, std::string& err) {
             t.ew[row * n + q] = w;
             t.eg[(row * 2 + 0) * n + q] = w * (c0 * a[0 * P2 + p2] + c1 * a[2 * P2 + p2]);
             t.eg[(row * 2 + 1) * n + q] = w * (c0 * a[1 * P2 + p2] + c1 * a[3 * P2 + p2]);
+            for (int o = 0; o < 2; ++o) {
+              const double ct = RC(rt.src_face, rt.src_edge, l, qs, o, 0), cp = RC(rt.src_face, rt.src_edge, l, qs, o, 1);
+              t.egc[((row * 2 + o) * 2 + 0) * n + q] = w * (ct * a[0 * P2 + p2] + cp * a[2 * P2 + p2]);
+              t.egc[((row * 2 + o) * 2 + 1) * n + q] = w * (ct * a[1 * P2 + p2] + cp * a[3 * P2 + p2]);
+            }
           }
         }
       }

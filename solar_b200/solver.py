@@ -183,6 +183,13 @@ class Solver:
         _lib.check(self.lib.solar_gpu_divergence(self._h, _ptr(a[0]), _ptr(a[1]), _ptr(a[2]), _ptr(out)))
         return out
 
+    def curl(self, axi: np.ndarray, aeta: np.ndarray, ar: np.ndarray):
+        """COMPUTE_CURL (grad.f90:140-255): returns (curl_xi, curl_eta, curl_r)."""
+        a = [np.ascontiguousarray(x, dtype=np.float64) for x in (axi, aeta, ar)]
+        out = [np.empty(self.field_shape) for _ in range(3)]
+        _lib.check(self.lib.solar_gpu_curl(self._h, *(_ptr(x) for x in a), *(_ptr(x) for x in out)))
+        return tuple(out)
+
     # ------------------------------------------------------------------ diagnostics
     def norm(self, field: int = 4, run: int = 0) -> float:
         out = ctypes.c_double()
