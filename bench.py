@@ -340,6 +340,36 @@ def split_block(cfg, args, world, local):
             "ms_per_step": ms / args.steps, "zones_per_rank": 6 // world, "norm_vr": norm}
 
 
+def large_adjoint_block(device: int, nsteps: int, outer: int, inner: int):
+    """Misfit gradient on the large grid (6 x 384^3 stratified shell, 16 sources, FP32 4
+    fields, one receiver 0.02 above each source, zero data so J = 1/2 sum p^2): two
+    checkpoint levels keep it inside one GPU's memory."""
+    import numpy as np
+    import torch
+
+    from solar_b200 import configs, receivers
+    from solar_b200.solver import Solver
+
+    cfg = configs.c5(nsteps=nsteps)
+    pts = [np.asarray(s.x0) / np.linalg.norm(s.x0) * 0.97 for s in cfg.sources]
+    loc = receivers.locate(cfg, pts)
+    with Solver(cfg, precision="fp32", nfields=4, device=device) as s:
+        s.init_sources()
+        s.set_receivers(loc)
+        res = s.misfit_gradient(nsteps, outer, np.zeros((nsteps, len(loc))), inner_every=inner)
+        free, total = torch.cuda.mem_get_info(device)
+    g = res["grad_c"]
+    total_ms = res["forward_ms"] + res["recompute_ms"] + res["adjoint_ms"]
+    return {"workload": "c5: 6 x %d^3 stratified shell, %d steps, %d receivers, FP32 F=4, checkpoints every %d "
+                        "steps with inner checkpoints every %d" % (cfg.nx, nsteps, len(loc), outer, inner),
+            "misfit": res["misfit"], "gradient_ms": total_ms, "forward_ms": res["forward_ms"],
+            "recompute_ms": res["recompute_ms"], "adjoint_ms": res["adjoint_ms"],
+            "adjoint_pt_steps_per_s": cfg.points * nsteps / (res["adjoint_ms"] / 1e3),
+            "gradient_cost_in_forward_runs": total_ms / res["forward_ms"],
+            "device_memory_in_use_gb": (total - free) / 1e9, "grad_finite": bool(np.isfinite(g).all()),
+            "grad_norm": float(np.linalg.norm(g))}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -358,6 +388,8 @@ def main():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-large", action="store_true")
     ap.add_argument("--large-steps", type=int, default=200)
+    ap.add_argument("--large-adjoint", action="store_true",
+                    help="also run the misfit gradient on the 6 x 384^3 grid (about 160 GB of device memory)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -448,6 +480,9 @@ def main():
         batch = batch_block(local)
     if world == 1 and not args.no_large:
         large = large_block(local, args.large_steps)
+    large_adj = None
+    if world == 1 and args.large_adjoint:
+        large_adj = large_adjoint_block(local, args.large_steps, 20, 4)
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(cfg, 2)
@@ -481,6 +516,7 @@ def main():
         "adjoint": adjoint,
         "batched_sources": batch,
         "large_grid": large,
+        "large_grid_adjoint": large_adj,
         "zone_split": split,
     }
     print(json.dumps(line), flush=True)

@@ -288,6 +288,16 @@ int solar_gpu_record(solar_ctx* c, int nsteps, double* traces);
 int solar_gpu_misfit_gradient(solar_ctx* c, int nsteps, int checkpoint_every, const double* data,
                               double* misfit, double* grad_c, double* lambda0, double* times_ms);
 
+/* solar_gpu_misfit_gradient with two checkpoint levels, for grids whose single-level
+ * checkpoints do not fit: states are kept every checkpoint_every steps for the whole run;
+ * each of those segments is run forward once more keeping a state every inner_every steps,
+ * and only those inner segments store stage divergences (memory: one state per outer and
+ * per inner checkpoint plus 5 * inner_every field volumes; cost: one more forward run).
+ * inner_every >= checkpoint_every is the single-level sweep. */
+int solar_gpu_misfit_gradient_nested(solar_ctx* c, int nsteps, int checkpoint_every, int inner_every,
+                                     const double* data, double* misfit, double* grad_c, double* lambda0,
+                                     double* times_ms);
+
 /* out = L^T mu, L(q) = SPONGE(BC_RHS(COMPUTE_RHS(q))) as a linear map of the state. */
 int solar_gpu_rhs_adjoint(solar_ctx* c, const double* mu, double* out);
 

@@ -77,6 +77,7 @@ EXPORTS = {
     "solar_gpu_set_receivers": [_P, ctypes.c_int, _D],
     "solar_gpu_record": [_P, ctypes.c_int, _D],
     "solar_gpu_misfit_gradient": [_P, ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _D],
+    "solar_gpu_misfit_gradient_nested": [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _D],
     "solar_gpu_rhs_adjoint": [_P, _D, _D],
     "solar_gpu_filter_adjoint": [_P, _D, _D],
     "solar_gpu_rk4_adjoint": [_P, ctypes.c_int, _D, _D],

@@ -158,21 +158,31 @@ static void enqueue_sample(solar_ctx* c, double* out) {
   sample_kernel<T><<<blocks_for(b.nrec, 128), 128, 0, c->stream>>>((const T*)c->A, b.rec_off, b.rec_w, b.nrec, out);
 }
 
+// The checkpointed sweep.  Outer checkpoints every K steps are kept for the whole run.  With
+// K2 < K each outer segment is first run forward again keeping inner checkpoints every K2
+// steps, and each inner segment is then recomputed storing its stage-input divergences and
+// reversed; memory is one state per outer and per inner checkpoint plus 5 * K2 field volumes,
+// for one more forward run than the single-level sweep (K2 = K).
 template <typename T>
-static int misfit_gradient_t(solar_ctx* c, int N, int K, const double* data, double* misfit, double* grad_c,
+static int misfit_gradient_t(solar_ctx* c, int N, int K, int K2, const double* data, double* misfit, double* grad_c,
                              double* lambda0, double* times) {
   AdjBuffers& b = c->adj;
   const long long V6 = 6 * vol_compact(c);
   const size_t S = (size_t)state_bytes(c);
   const int ncp = (N + K - 1) / K;
+  K2 = std::max(1, std::min(K2, K));
+  const int nsub_max = (std::min(K, N) + K2 - 1) / K2;
   int rc;
   if ((rc = adj_reserve(&b.ckpt, &b.ckpt_bytes, S * (size_t)ncp))) return rc;
-  if ((rc = adj_reserve(&b.div, &b.div_bytes, (size_t)std::min(K, N) * 5 * V6 * sizeof(T)))) return rc;
+  if (nsub_max > 1 && (rc = adj_reserve(&b.ckpt2, &b.ckpt2_bytes, S * (size_t)nsub_max))) return rc;
+  if ((rc = adj_reserve(&b.div, &b.div_bytes, (size_t)std::min(K2, N) * 5 * V6 * sizeof(T)))) return rc;
   if ((rc = adj_reserve((void**)&b.traces, &b.traces_bytes, (size_t)std::max(N, 1) * b.nrec * 2 * sizeof(double)))) return rc;
   // with a source term the clock (time, step, interpolation state) is checkpointed too
   const size_t CL = sizeof(ForceClock);
-  if (c->forcing && (rc = adj_reserve(&b.clk, &b.clk_bytes, CL * (size_t)ncp))) return rc;
+  if (c->forcing && (rc = adj_reserve(&b.clk, &b.clk_bytes, CL * (size_t)(ncp + nsub_max)))) return rc;
   char* clk = (char*)b.clk;
+  char* clk2 = clk + CL * (size_t)ncp;
+  char* ckpt2 = (char*)b.ckpt2;
   double* traces = b.traces;
   double* res = b.traces + (size_t)N * b.nrec;
   char* ckpt = (char*)b.ckpt;
@@ -206,25 +216,48 @@ static int misfit_gradient_t(solar_ctx* c, int N, int K, const double* data, dou
   float t_rec = 0.f, t_adj = 0.f;
   for (int seg = ncp - 1; seg >= 0; --seg) {
     const int n0 = seg * K, n1 = std::min(N, n0 + K);
+    const int nsub = (n1 - n0 + K2 - 1) / K2;
     CK(cudaEventRecord(c->ev[4], c->stream));
     CK(cudaMemcpyAsync(c->A, ckpt + (size_t)seg * S, S, cudaMemcpyDeviceToDevice, c->stream));
     if (c->forcing) CK(cudaMemcpyAsync(c->force_clock, clk + (size_t)seg * CL, CL, cudaMemcpyDeviceToDevice, c->stream));
-    for (int n = n0; n < n1; ++n)
-      if ((rc = enqueue_step_div<T>(c, D + (size_t)(n - n0) * 5 * V6))) return rc;
-    CK(cudaEventRecord(c->ev[5], c->stream));
-    for (int n = n1; n > n0; --n) {
-      // lambda += S^T (S q_n - d_n), then lambda <- STEP^T lambda (with the gradient)
-      inject_kernel<T><<<blocks_for(b.nrec, 128), 128, 0, c->stream>>>((T*)c->adj.L, b.rec_off, b.rec_w, b.nrec,
-                                                                        res + (size_t)(n - 1) * b.nrec);
-      if ((rc = enqueue_step_adjoint<T>(c, D + (size_t)(n - 1 - n0) * 5 * V6, b.grad))) return rc;
+    if (nsub > 1)                  // inner checkpoints of this segment
+      for (int n = n0; n < n1; ++n) {
+        if ((n - n0) % K2 == 0) {
+          const size_t q = (size_t)((n - n0) / K2);
+          CK(cudaMemcpyAsync(ckpt2 + q * S, c->A, S, cudaMemcpyDeviceToDevice, c->stream));
+          if (c->forcing) CK(cudaMemcpyAsync(clk2 + q * CL, c->force_clock, CL, cudaMemcpyDeviceToDevice, c->stream));
+        }
+        CK(cudaGraphLaunch(c->step_graph, c->stream));
+      }
+    CK(cudaEventRecord(c->ev[7], c->stream));
+    CK(cudaEventSynchronize(c->ev[7]));
+    float r0 = 0.f;
+    CK(cudaEventElapsedTime(&r0, c->ev[4], c->ev[7]));
+    t_rec += r0;
+    for (int sub = nsub - 1; sub >= 0; --sub) {
+      const int m0 = n0 + sub * K2, m1 = std::min(n1, m0 + K2);
+      CK(cudaEventRecord(c->ev[4], c->stream));
+      if (nsub > 1) {
+        CK(cudaMemcpyAsync(c->A, ckpt2 + (size_t)sub * S, S, cudaMemcpyDeviceToDevice, c->stream));
+        if (c->forcing) CK(cudaMemcpyAsync(c->force_clock, clk2 + (size_t)sub * CL, CL, cudaMemcpyDeviceToDevice, c->stream));
+      }
+      for (int n = m0; n < m1; ++n)
+        if ((rc = enqueue_step_div<T>(c, D + (size_t)(n - m0) * 5 * V6))) return rc;
+      CK(cudaEventRecord(c->ev[5], c->stream));
+      for (int n = m1; n > m0; --n) {
+        // lambda += S^T (S q_n - d_n), then lambda <- STEP^T lambda (with the gradient)
+        inject_kernel<T><<<blocks_for(b.nrec, 128), 128, 0, c->stream>>>((T*)c->adj.L, b.rec_off, b.rec_w, b.nrec,
+                                                                          res + (size_t)(n - 1) * b.nrec);
+        if ((rc = enqueue_step_adjoint<T>(c, D + (size_t)(n - 1 - m0) * 5 * V6, b.grad))) return rc;
+      }
+      CK(cudaEventRecord(c->ev[6], c->stream));
+      CK(cudaEventSynchronize(c->ev[6]));
+      float a = 0.f, r = 0.f;
+      CK(cudaEventElapsedTime(&r, c->ev[4], c->ev[5]));
+      CK(cudaEventElapsedTime(&a, c->ev[5], c->ev[6]));
+      t_rec += r;
+      t_adj += a;
     }
-    CK(cudaEventRecord(c->ev[6], c->stream));
-    CK(cudaEventSynchronize(c->ev[6]));
-    float a = 0.f, r = 0.f;
-    CK(cudaEventElapsedTime(&r, c->ev[4], c->ev[5]));
-    CK(cudaEventElapsedTime(&a, c->ev[5], c->ev[6]));
-    t_rec += r;
-    t_adj += a;
   }
   // leave the state (and the clock) at the initial condition
   CK(cudaMemcpyAsync(c->A, ckpt, S, cudaMemcpyDeviceToDevice, c->stream));
@@ -308,13 +341,21 @@ int solar_gpu_record(solar_ctx* c, int nsteps, double* traces) {
 
 int solar_gpu_misfit_gradient(solar_ctx* c, int nsteps, int checkpoint_every, const double* data,
                               double* misfit, double* grad_c, double* lambda0, double* times_ms) {
+  return solar_gpu_misfit_gradient_nested(c, nsteps, checkpoint_every, checkpoint_every, data, misfit, grad_c,
+                                          lambda0, times_ms);
+}
+
+int solar_gpu_misfit_gradient_nested(solar_ctx* c, int nsteps, int checkpoint_every, int inner_every,
+                                     const double* data, double* misfit, double* grad_c, double* lambda0,
+                                     double* times_ms) {
   int rc = check_ctx(c);
   if (rc) return rc;
+  if (inner_every < 1) return fail(SOLAR_ERR_ARG, "need inner_every >= 1");
   if (nsteps < 1 || checkpoint_every < 1 || !data) return fail(SOLAR_ERR_ARG, "need nsteps >= 1, checkpoint_every >= 1 and data");
   if (!c->adj.nrec) return fail(SOLAR_ERR_STATE, "no receivers set");
   if ((rc = adj_alloc(c))) return rc;
-  return c->fp32 ? misfit_gradient_t<float>(c, nsteps, checkpoint_every, data, misfit, grad_c, lambda0, times_ms)
-                 : misfit_gradient_t<double>(c, nsteps, checkpoint_every, data, misfit, grad_c, lambda0, times_ms);
+  return c->fp32 ? misfit_gradient_t<float>(c, nsteps, checkpoint_every, inner_every, data, misfit, grad_c, lambda0, times_ms)
+                 : misfit_gradient_t<double>(c, nsteps, checkpoint_every, inner_every, data, misfit, grad_c, lambda0, times_ms);
 }
 
 int solar_gpu_rhs_adjoint(solar_ctx* c, const double* mu, double* out) {

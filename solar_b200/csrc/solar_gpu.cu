@@ -67,6 +67,8 @@ struct AdjBuffers {
   double* grad = nullptr;   // dJ/dc, compact [face][k][j][i]
   void* ckpt = nullptr;     // state checkpoints (padded copies of the state buffer)
   size_t ckpt_bytes = 0;
+  void* ckpt2 = nullptr;    // inner checkpoints of one outer segment (nested sweep)
+  size_t ckpt2_bytes = 0;
   void* div = nullptr;      // stage-input divergences of one checkpoint segment
   size_t div_bytes = 0;
   void* clk = nullptr;      // source-term clocks of the checkpoints
@@ -544,7 +546,7 @@ int solar_gpu_finalize(solar_ctx* c) {
                   c->dt.rad64, c->dt.vol2, c->dt.drw, c->dt.c2_64, c->dt.tanx, c->dt.gr};
   for (void* p : ptrs)
     if (p) cudaFree(p);
-  void* aptrs[] = {c->adj.L, c->adj.LW, c->adj.T1, c->adj.T2, c->adj.rb, c->adj.grad, c->adj.ckpt,
+  void* aptrs[] = {c->adj.L, c->adj.LW, c->adj.T1, c->adj.T2, c->adj.rb, c->adj.grad, c->adj.ckpt, c->adj.ckpt2,
                    c->adj.div, c->adj.traces, c->adj.rec_off, c->adj.rec_w, c->adj.clk, c->split_items, c->split_slots,
                    c->force_clock, c->force_exy, c->force_samples, c->force_xy, c->force_r};
   for (void* p : aptrs)

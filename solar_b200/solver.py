@@ -275,8 +275,9 @@ class Solver:
         return out
 
     def misfit_gradient(self, nsteps: int, checkpoint_every: int, data: np.ndarray,
-                        want_lambda: bool = False) -> dict:
-        """Misfit of the receiver traces against ``data`` (nsteps, nrec) and dJ/dc per point."""
+                        want_lambda: bool = False, inner_every: Optional[int] = None) -> dict:
+        """Misfit of the receiver traces against ``data`` (nsteps, nrec) and dJ/dc per point.
+        ``inner_every`` < ``checkpoint_every`` selects the two-level checkpointed sweep."""
         data = np.ascontiguousarray(data, dtype=np.float64)
         if data.shape != (int(nsteps), self.nrec):
             raise ValueError(f"data must have shape {(int(nsteps), self.nrec)}")
@@ -284,8 +285,9 @@ class Solver:
         grad = np.empty(self.field_shape)
         lam = np.empty(self.state_shape) if want_lambda else None
         times = (ctypes.c_double * 3)()
-        _lib.check(self.lib.solar_gpu_misfit_gradient(
-            self._h, int(nsteps), int(checkpoint_every), _ptr(data), ctypes.byref(J), _ptr(grad),
+        inner = int(checkpoint_every if inner_every is None else inner_every)
+        _lib.check(self.lib.solar_gpu_misfit_gradient_nested(
+            self._h, int(nsteps), int(checkpoint_every), inner, _ptr(data), ctypes.byref(J), _ptr(grad),
             _ptr(lam) if lam is not None else None, times))
         out = {"misfit": J.value, "grad_c": grad,
                "forward_ms": times[0], "recompute_ms": times[1], "adjoint_ms": times[2]}

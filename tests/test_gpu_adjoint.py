@@ -256,6 +256,22 @@ def test_checkpoint_interval_does_not_change_gradient(c2_case):
     assert np.linalg.norm(g1 - g0) <= 1e-12 * np.linalg.norm(g0)
 
 
+@pytest.mark.parametrize("outer,inner", [(10, 3), (24, 5), (7, 1)])
+def test_nested_checkpoints_give_the_same_gradient(c2_case, outer, inner):
+    """Two checkpoint levels (ragged outer and inner segments included) reproduce the
+    single-level sweep."""
+    cs = c2_case
+    with Solver(cs["cfg"], c2_3d=cs["c0"] ** 2) as s:
+        s.set_state(cs["q0"])
+        s.set_receivers(cs["loc"])
+        r = s.misfit_gradient(cs["nsteps"], outer, cs["data"], want_lambda=True, inner_every=inner)
+        np.testing.assert_array_equal(s.get_state(), cs["q0"])
+    g0 = cs["res"]["grad_c"]
+    assert r["misfit"] == cs["res"]["misfit"]
+    assert np.linalg.norm(r["grad_c"] - g0) <= 1e-12 * np.linalg.norm(g0)
+    assert np.linalg.norm(r["lambda0"] - cs["res"]["lambda0"]) <= 1e-12 * np.linalg.norm(cs["res"]["lambda0"])
+
+
 def test_state_is_restored_after_gradient(c2s, c2_case):
     cs = c2_case
     with Solver(c2s, c2_3d=cs["c0"] ** 2) as s:
