@@ -25,22 +25,25 @@
 
 namespace solar {
 
-// Fused transposed stage: adj_pre_kernel + adj_deriv_kernel in one pass over the state.
-// A CTA owns a TX x TY column tile of one face and marches the planes of its chunk (plus
-// three planes on either side for the radial window).  Per plane it forms the
-// coefficient-weighted volumes X1, X2 (on the tile and its xi halo) and Y1, Y2 (tile and
-// eta halo) in shared memory from mu = lw + beta lq of that plane (zero outside the face
-// and on the BC planes), applies -D_xi / -D_eta, and keeps facr * R1 and facr * R2 of the
-// last seven planes in registers for the banded part of the radial transpose, which
-// completes plane k three iterations later.  The rows of the one-sided radial stencil
-// (planes 1, 2, nr-3, nr-2; planes 0 and nr-1 carry zero) are written to `rb` and
-// added by adj_rbdy_kernel.  Edge tiles also write the ghost-frame adjoints.  Inputs
-// (lq, lw) and outputs (lout, lwout) are distinct buffers: neighbouring CTAs read the
+// Fused transposed stage (pointwise part + transposed stencils in one pass).  A CTA owns a
+// TX x TY column tile of one face and marches the planes of its chunk (plus three planes on
+// either side for the radial window).  Planes stream in through TMA tile loads into a ring of
+// shared-memory slots, each guarded by an mbarrier: for a plane of the chunk, the lambda_q
+// and lambda_w boxes (tile plus a 4-column / 3-row halo) of v_xi, v_eta, p and rho and the
+// tiles of v_r; for the three extra planes on either side only the tiles of p, rho and v_r.
+// Per plane the kernel forms the coefficient-weighted volumes X1, X2 (on the tile and its
+// xi halo) and Y1, Y2 (tile and eta halo) in shared memory from mu = lw + beta lq (zero
+// outside the face and on the BC planes), applies -D_xi / -D_eta, and keeps facr * R1 and
+// facr * R2 of the last seven planes in registers for the banded part of the radial
+// transpose, which completes plane k three iterations later.  The rows of the one-sided
+// radial stencil (planes 1, 2, nr-3, nr-2; planes 0 and nr-1 carry zero) are written to
+// `rb` and added by adj_rbdy_kernel.  Edge tiles also write the ghost-frame adjoints.
+// Inputs (lq, lw) and outputs (lout, lwout) are distinct buffers: neighbouring CTAs read the
 // inputs' halos.
 template <typename T>
 struct AdjStageArgs {
-  const T* lq;
-  const T* lw;
+  CUtensorMap mBq, mBw;   // boxes (TX+8) x (TY+6) of lq / lw
+  CUtensorMap mTq, mTw;   // tiles TX x TY of lq / lw
   T* lout;
   T* lwout;
   T* rb;              // [face][4][2][n*n] raw R1, R2 of planes 1, 2, nr-3, nr-2
@@ -49,17 +52,36 @@ struct AdjStageArgs {
   double* grad;
   const T* rad;
   const T* met;
+  int* err;
   Geom g;
   T alpha, beta, dt, inv_dxi;
   int keep, kchunk;
 };
 
+template <typename T> struct AdjRing { static constexpr int value = sizeof(T) == 8 ? 2 : 3; };
+
 template <typename T, int TX, int TY>
-__global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const AdjStageArgs<T> a) {
-  constexpr int XW = TX + 6, YH = TY + 6;
+struct AdjLayout {
+  static constexpr int PW = TX + 8, PH = TY + 6, PB = PW * PH, OB = TX * TY;
+  static constexpr size_t P_BYTES = align128(PB * sizeof(T));
+  static constexpr size_t O_BYTES = align128(OB * sizeof(T));
+  // a chunk plane: boxes [v_xi, v_eta, p, rho] x [lq, lw], then the v_r tiles [lq, lw];
+  // an extra plane: tiles [p, rho, v_r] x [lq, lw] from the slot's start
+  static constexpr size_t SLOT = 8 * P_BYTES + 2 * O_BYTES;
+  static constexpr int RING = AdjRing<T>::value;
+  static constexpr size_t BAR = RING * SLOT;
+  static constexpr size_t TOTAL = BAR + RING * sizeof(uint64_t);
+};
+
+template <typename T, int TX, int TY>
+__global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const __grid_constant__ AdjStageArgs<T> a) {
+  using L = AdjLayout<T, TX, TY>;
+  constexpr int XW = TX + 6, YH = TY + 6, PW = L::PW;
   constexpr int NHALO = 6 * TX + 6 * TY;
   static_assert(NHALO <= TX * TY, "one halo point per thread");
   __shared__ T sX1[TY][XW], sX2[TY][XW], sY1[YH][TX], sY2[YH][TX];
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L::BAR);
   const Geom& g = a.g;
   const int n = g.n, nr = g.nr;
   const long long P2 = (long long)n * n;
@@ -72,68 +94,114 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const AdjStageArg
   const int i = i0 + tx, j = j0 + ty;
   const int p2 = j * n + i;
   const int sRho = g.slot[kRho], sX = g.slot[kVxi], sY = g.slot[kVeta], sR = g.slot[kVr], sP = g.slot[kP];
-  const T* __restrict__ lq = a.lq;
-  const T* __restrict__ lw = a.lw;
+  const bool has_rho = sRho >= 0;
   const T* __restrict__ met = a.met;
   const T* __restrict__ rad = a.rad;
-  const T tD = __ldg(met + mD * P2 + p2), tXYD = __ldg(met + mXYD * P2 + p2), tC = __ldg(met + mC * P2 + p2);
-  const T tXYC = __ldg(met + mXYC * P2 + p2), tDivX = __ldg(met + mDivX * P2 + p2), tDivY = __ldg(met + mDivY * P2 + p2);
-  const T tTX = __ldg(met + mTX * P2 + p2), tTY = __ldg(met + mTY * P2 + p2);
   const T c1 = Coef<T>::drp(1), c2c = Coef<T>::drp(2), c3 = Coef<T>::drp(3);
   // this thread's halo point: eta-halo rows first, then xi-halo columns
-  bool has_halo = tid < NHALO, xi_halo = false;
+  const bool has_halo = tid < NHALO;
+  bool xi_halo = false;
   int hi = 0, hj = 0;
   if (tid < 6 * TX) { hi = tid % TX; const int r = tid / TX; hj = r < 3 ? r - 3 : TY + r - 3; }
   else if (has_halo) { xi_halo = true; const int q = tid - 6 * TX; hj = q % TY; const int cc = q / TY; hi = cc < 3 ? cc - 3 : TX + cc - 3; }
   const int hgi = i0 + hi, hgj = j0 + hj;
   const bool h_in = has_halo && hgi >= 0 && hgi < n && hgj >= 0 && hgj < n;
   const int hq2 = h_in ? hgj * n + hgi : 0;
-  T hm1 = T(0), hm2 = T(0);       // halo point metric: (D, XY/C, DivX) for xi, (XY/D, C, DivY) for eta
-  T hm3 = T(0);
-  if (h_in) {
-    hm1 = __ldg(met + (xi_halo ? mD : mXYD) * P2 + hq2);
-    hm2 = __ldg(met + (xi_halo ? mXYC : mC) * P2 + hq2);
-    hm3 = __ldg(met + (xi_halo ? mDivX : mDivY) * P2 + hq2);
+  // 32-bit offsets inside one field volume; the field bases of this face are formed once
+  T* const lo_face = a.lout + g.vol(0, face, 0);
+  T* const lw_face = a.lwout + g.vol(0, face, 0);
+  const int vs = (int)g.vs, plane = (int)g.plane;
+  auto fo = [&](int s) { return s * vs; };                          // field base (elements)
+  const int own0 = (JOFF + j) * g.pitch + IOFF + i;                 // own point in plane 0
+  const int face_c2 = face * nr;                                    // plane index base, compact arrays
+  // planes loaded through the ring: every real plane of [kb-3, ke+2]
+  const int m_lo = max(kb - 3, 0), m_hi = min(ke + 2, nr - 1);
+  const int zf = face * g.nf;            // plane index of (slot s, k) = (zf + s) * nr + k (run 0)
+  const int xB = IOFF + i0 - 4, yB = JOFF + j0 - 3, xT = IOFF + i0, yT = JOFF + j0;
+  auto slot_base = [&](int sl) { return smem + (size_t)sl * L::SLOT; };
+  auto issue = [&](int m, int sl) {
+    uint64_t* bar = &bars[sl];
+    unsigned char* base = slot_base(sl);
+    if (m >= kb && m < ke) {
+      const int nbox = has_rho ? 4 : 3;
+      mbar_expect_tx(bar, (uint32_t)((2 * nbox * L::PB + 2 * L::OB) * sizeof(T)));
+      const int bs[4] = {sX, sY, sP, sRho};
+      for (int f = 0; f < nbox; ++f) {
+        tma_load_3d(base + (2 * f) * L::P_BYTES, &a.mBq, xB, yB, (zf + bs[f]) * nr + m, bar);
+        tma_load_3d(base + (2 * f + 1) * L::P_BYTES, &a.mBw, xB, yB, (zf + bs[f]) * nr + m, bar);
+      }
+      tma_load_3d(base + 8 * L::P_BYTES, &a.mTq, xT, yT, (zf + sR) * nr + m, bar);
+      tma_load_3d(base + 8 * L::P_BYTES + L::O_BYTES, &a.mTw, xT, yT, (zf + sR) * nr + m, bar);
+    } else {
+      const int nt = has_rho ? 3 : 2;
+      mbar_expect_tx(bar, (uint32_t)(2 * nt * L::OB * sizeof(T)));
+      const int ts[3] = {sP, sR, sRho};
+      for (int f = 0; f < nt; ++f) {
+        tma_load_3d(base + (2 * f) * L::O_BYTES, &a.mTq, xT, yT, (zf + ts[f]) * nr + m, bar);
+        tma_load_3d(base + (2 * f + 1) * L::O_BYTES, &a.mTw, xT, yT, (zf + ts[f]) * nr + m, bar);
+      }
+    }
+  };
+  if (tid == 0) {
+    for (int q = 0; q < L::RING; ++q) mbar_init(&bars[q], 1);
+    mbar_fence_init();
   }
-  auto vol = [&](int s) { return g.vol(0, face, s); };
+  __syncthreads();
+  int m_issued = m_lo;
+  if (tid == 0) {
+    tma_prefetch_desc(&a.mBq);
+    tma_prefetch_desc(&a.mBw);
+    for (int q = 0; q < L::RING && m_issued <= m_hi; ++q, ++m_issued) issue(m_issued, q);
+  }
   T w1[7], w2[7];          // facr * R1, facr * R2 of planes m-6 .. m (banded rows only)
   T pp[4], pv[4];          // partial outputs of p and v_r, planes m-3 .. m
 #pragma unroll
   for (int q = 0; q < 7; ++q) { w1[q] = T(0); w2[q] = T(0); }
 #pragma unroll
   for (int q = 0; q < 4; ++q) { pp[q] = T(0); pv[q] = T(0); }
+  int slot = 0;
+  uint32_t phase = 0;
+  bool ok = true;
+  const int bo = (ty + 3) * PW + tx + 4;           // own point in a box
+  const int to = ty * TX + tx;                     // own point in a tile
   for (int m = kb - 3; m <= ke + 2; ++m) {
     const bool real = (m >= 0 && m < nr);
     const bool own = (m >= kb && m < ke);
     const bool bc = (m == 0 || m == nr - 1);
     T r1 = T(0), r2 = T(0), part_p = T(0), part_v = T(0);
     if (real) {
-      const long long o = g.at(m, j, i);
-      const long long plane_c2 = ((long long)face * nr + m) * P2;
-      // ---- every global load of this plane first
-      T lqv[5], lwv[5];
-#pragma unroll
-      for (int f = 0; f < 5; ++f) {
-        const int s = g.slot[f];
-        const bool need = s >= 0 && (own || f == kVr || f == kP || f == kRho);
-        lqv[f] = need ? __ldg(lq + vol(s) + o) : T(0);
-        lwv[f] = need ? __ldg(lw + vol(s) + o) : T(0);
-      }
-      T hx = T(0), hy = T(0), hp = T(0), hr = T(0), hc2 = T(0);
-      const bool do_halo = own && h_in && !bc;
-      if (do_halo) {
-        const long long oh = g.at(m, hgj, hgi);
-        hx = __ldg(lw + vol(sX) + oh) + a.beta * __ldg(lq + vol(sX) + oh);
-        hy = __ldg(lw + vol(sY) + oh) + a.beta * __ldg(lq + vol(sY) + oh);
-        hp = __ldg(lw + vol(sP) + oh) + a.beta * __ldg(lq + vol(sP) + oh);
-        if (sRho >= 0) hr = __ldg(lw + vol(sRho) + oh) + a.beta * __ldg(lq + vol(sRho) + oh);
-        if (a.c2) hc2 = __ldg(a.c2 + plane_c2 + hq2);
-      }
+      const int o = m * plane + own0;
+      const long long plane_c2 = (long long)(face_c2 + m) * P2;
+      // global loads that do not come through the ring
       const T c2own = a.c2 ? __ldg(a.c2 + plane_c2 + p2) : T(0);
       const T divv = (own && a.grad) ? __ldg(a.div + plane_c2 + p2) : T(0);
+      const bool do_halo = own && h_in && !bc;
+      const T hc2 = (do_halo && a.c2) ? __ldg(a.c2 + plane_c2 + hq2) : T(0);
       const T invr = __ldg(rad + rInvR * nr + m), inv_rho0 = __ldg(rad + rInvRho0 * nr + m);
       const T rho0 = __ldg(rad + rRho0 * nr + m), c2r = __ldg(rad + rC2Rho0 * nr + m);
-      // ---- compute
+      ok &= mbar_wait(&bars[slot], phase, a.err, 5);
+      const T* sb = reinterpret_cast<const T*>(slot_base(slot));
+      constexpr int PBs = (int)(L::P_BYTES / sizeof(T)), OBs = (int)(L::O_BYTES / sizeof(T));
+      T lqv[5], lwv[5];
+#pragma unroll
+      for (int f = 0; f < 5; ++f) { lqv[f] = T(0); lwv[f] = T(0); }
+      if (own) {
+        const int bf[4] = {kVxi, kVeta, kP, kRho};
+#pragma unroll
+        for (int f = 0; f < 4; ++f) {
+          if (f == 3 && !has_rho) continue;
+          lqv[bf[f]] = sb[(2 * f) * PBs + bo];
+          lwv[bf[f]] = sb[(2 * f + 1) * PBs + bo];
+        }
+        lqv[kVr] = sb[8 * PBs + to];
+        lwv[kVr] = sb[8 * PBs + OBs + to];
+      } else {
+        lqv[kP] = sb[to];
+        lwv[kP] = sb[OBs + to];
+        lqv[kVr] = sb[2 * OBs + to];
+        lwv[kVr] = sb[3 * OBs + to];
+        if (has_rho) { lqv[kRho] = sb[4 * OBs + to]; lwv[kRho] = sb[5 * OBs + to]; }
+      }
       T mu[5], mp[5];
 #pragma unroll
       for (int f = 0; f < 5; ++f) {
@@ -145,14 +213,27 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const AdjStageArg
       r1 = -inv_rho0 * mp[kVr];
       r2 = e;
       if (own) {
+        const T tD = __ldg(met + mD * P2 + p2), tXYD = __ldg(met + mXYD * P2 + p2), tC = __ldg(met + mC * P2 + p2);
+        const T tXYC = __ldg(met + mXYC * P2 + p2);
         sX1[ty][tx + 3] = -invr * inv_rho0 * (tD * mp[kVxi] + tXYC * mp[kVeta]);
-        sX2[ty][tx + 3] = invr * tDivX * e;
+        sX2[ty][tx + 3] = invr * __ldg(met + mDivX * P2 + p2) * e;
         sY1[ty + 3][tx] = -invr * inv_rho0 * (tXYD * mp[kVxi] + tC * mp[kVeta]);
-        sY2[ty + 3][tx] = invr * tDivY * e;
+        sY2[ty + 3][tx] = invr * __ldg(met + mDivY * P2 + p2) * e;
         if (has_halo) {
-          const T he = -(a.c2 ? hc2 * rho0 : c2r) * hp - rho0 * hr;
-          const T v1 = do_halo ? -invr * inv_rho0 * (hm1 * hx + hm2 * hy) : T(0);
-          const T v2 = do_halo ? invr * hm3 * he : T(0);
+          T v1 = T(0), v2 = T(0);
+          if (do_halo) {
+            const int hb = (hj + 3) * PW + hi + 4;
+            const T hx = sb[1 * PBs + hb] + a.beta * sb[0 * PBs + hb];
+            const T hy = sb[3 * PBs + hb] + a.beta * sb[2 * PBs + hb];
+            const T hp = sb[5 * PBs + hb] + a.beta * sb[4 * PBs + hb];
+            const T hr = has_rho ? sb[7 * PBs + hb] + a.beta * sb[6 * PBs + hb] : T(0);
+            const T he = -(a.c2 ? hc2 * rho0 : c2r) * hp - rho0 * hr;
+            const T hm1 = __ldg(met + (xi_halo ? mD : mXYD) * P2 + hq2);
+            const T hm2 = __ldg(met + (xi_halo ? mXYC : mC) * P2 + hq2);
+            const T hm3 = __ldg(met + (xi_halo ? mDivX : mDivY) * P2 + hq2);
+            v1 = -invr * inv_rho0 * (hm1 * hx + hm2 * hy);
+            v2 = invr * hm3 * he;
+          }
           if (xi_halo) { sX1[hj][hi + 3] = v1; sX2[hj][hi + 3] = v2; }
           else { sY1[hj + 3][hi] = v1; sY2[hj + 3][hi] = v2; }
         }
@@ -160,8 +241,8 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const AdjStageArg
         const T sig = __ldg(rad + rSigma * nr + m);
         T pw[5];
         pw[kRho] = -__ldg(rad + rG0Rho0 * nr + m) * mp[kVr] - sig * mu[kRho];
-        pw[kVxi] = -invr * tTX * e;
-        pw[kVeta] = -invr * tTY * e;
+        pw[kVxi] = -invr * __ldg(met + mTX * P2 + p2) * e;
+        pw[kVeta] = -invr * __ldg(met + mTY * P2 + p2) * e;
         pw[kVr] = T(2) * invr * e - __ldg(rad + rDRho0 * nr + m) * mp[kRho] + __ldg(rad + rRho0G0 * nr + m) * mp[kP] -
                   sig * mu[kVr];
         pw[kP] = -sig * mu[kP];
@@ -169,11 +250,11 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const AdjStageArg
         for (int f = 0; f < 5; ++f) {
           const int s = g.slot[f];
           if (s < 0) continue;
-          a.lwout[vol(s) + o] = a.alpha * mu[f];
+          lw_face[fo(s) + o] = a.alpha * mu[f];
           const T base = (a.keep ? lqv[f] : T(0)) + a.dt * pw[f];
           if (f == kP) part_p = base;
           else if (f == kVr) part_v = base;
-          else if (f == kRho) a.lout[vol(s) + o] = base;
+          else if (f == kRho) lo_face[fo(s) + o] = base;
           else lqv[f] = base;                                  // v_xi, v_eta: 2-D part added below
         }
         if (a.grad) {
@@ -197,8 +278,8 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const AdjStageArg
         const T dy2 = c1 * (y2[TX] - y2[-TX]) + c2c * (y2[2 * TX] - y2[-2 * TX]) + c3 * (y2[3 * TX] - y2[-3 * TX]);
         const T k2 = -a.dt * a.inv_dxi;
         part_p += k2 * (dx1 + dy1);
-        a.lout[vol(sX) + o] = lqv[kVxi] + k2 * dx2;
-        a.lout[vol(sY) + o] = lqv[kVeta] + k2 * dy2;
+        lo_face[fo(sX) + o] = lqv[kVxi] + k2 * dx2;
+        lo_face[fo(sY) + o] = lqv[kVeta] + k2 * dy2;
         // ghost-frame adjoints of the neighbour faces' values (W/E columns, S/N rows)
         if ((i0 == 0 && tx < 3) || (i0 + TX == n && tx >= TX - 3)) {
           const bool west = i0 == 0 && tx < 3;
@@ -208,9 +289,9 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const AdjStageArg
           const T* r2p = &sX2[ty][0];
           const T f1 = c1 * (xv(r1p, c + 1) - xv(r1p, c - 1)) + c2c * (xv(r1p, c + 2) - xv(r1p, c - 2)) + c3 * (xv(r1p, c + 3) - xv(r1p, c - 3));
           const T f2 = c1 * (xv(r2p, c + 1) - xv(r2p, c - 1)) + c2c * (xv(r2p, c + 2) - xv(r2p, c - 2)) + c3 * (xv(r2p, c + 3) - xv(r2p, c - 3));
-          const long long og = g.at(m, j, west ? tx - 3 : n + (tx - (TX - 3)));
-          a.lout[vol(sP) + og] = k2 * f1;
-          a.lout[vol(sX) + og] = k2 * f2;
+          const int og = o - i + (west ? tx - 3 : n + (tx - (TX - 3)));
+          lo_face[fo(sP) + og] = k2 * f1;
+          lo_face[fo(sX) + og] = k2 * f2;
         }
         if ((j0 == 0 && ty < 3) || (j0 + TY == n && ty >= TY - 3)) {
           const bool south = j0 == 0 && ty < 3;
@@ -218,9 +299,9 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const AdjStageArg
           auto yv = [&](const T (*col)[TX], int q) { return (q >= 0 && q < YH) ? col[q][tx] : T(0); };
           const T f1 = c1 * (yv(sY1, r + 1) - yv(sY1, r - 1)) + c2c * (yv(sY1, r + 2) - yv(sY1, r - 2)) + c3 * (yv(sY1, r + 3) - yv(sY1, r - 3));
           const T f2 = c1 * (yv(sY2, r + 1) - yv(sY2, r - 1)) + c2c * (yv(sY2, r + 2) - yv(sY2, r - 2)) + c3 * (yv(sY2, r + 3) - yv(sY2, r - 3));
-          const long long og = g.at(m, south ? ty - 3 : n + (ty - (TY - 3)), i);
-          a.lout[vol(sP) + og] = k2 * f1;
-          a.lout[vol(sY) + og] = k2 * f2;
+          const int og = o + ((south ? ty - 3 : n + (ty - (TY - 3))) - j) * g.pitch;
+          lo_face[fo(sP) + og] = k2 * f1;
+          lo_face[fo(sY) + og] = k2 * f2;
         }
       }
     }
@@ -240,11 +321,20 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const AdjStageArg
       // (Dr^T R)_pl = sum_d a_d facr_{pl-d} R_{pl-d}, a_{-d} = -a_d; window index of pl-d is 3-d
       const T rp = c1 * (w1[2] - w1[4]) + c2c * (w1[1] - w1[5]) + c3 * (w1[0] - w1[6]);
       const T rv = c1 * (w2[2] - w2[4]) + c2c * (w2[1] - w2[5]) + c3 * (w2[0] - w2[6]);
-      const long long op = g.at(pl, j, i);
-      a.lout[vol(sP) + op] = pp[0] + a.dt * rp;
-      a.lout[vol(sR) + op] = pv[0] + a.dt * rv;
+      const int op = pl * plane + own0;
+      lo_face[fo(sP) + op] = pp[0] + a.dt * rp;
+      lo_face[fo(sR) + op] = pv[0] + a.dt * rv;
     }
-    if (own) __syncthreads();
+    if (real) {
+      // every thread is done with this slot (and with the X/Y arrays): refill it
+      if (__syncthreads_or(!ok)) break;
+      if (tid == 0 && m_issued <= m_hi) issue(m_issued++, slot);
+      if (++slot == L::RING) { slot = 0; phase ^= 1; }
+    }
+  }
+  if (!ok && tid == 0) {
+    // a wait gave up: give copies still in flight a bounded time to land before exit
+    for (int q = 0; q < 1000; ++q) __nanosleep(1000);
   }
 }
 

@@ -43,8 +43,6 @@ static int adj_reserve(void** p, size_t* have, size_t want) {
 template <typename T>
 static AdjStageArgs<T> adj_args(solar_ctx* c, double dt) {
   AdjStageArgs<T> a;
-  a.lq = nullptr;
-  a.lw = nullptr;
   a.lout = nullptr;
   a.lwout = nullptr;
   a.rb = nullptr;
@@ -60,6 +58,7 @@ static AdjStageArgs<T> adj_args(solar_ctx* c, double dt) {
   a.inv_dxi = (T)(1.0 / c->ht.dxi);
   a.keep = 0;
   a.kchunk = 0;
+  a.err = c->err;
   return a;
 }
 
@@ -69,24 +68,40 @@ static unsigned blocks_for(long long n, int threads) { return (unsigned)((n + th
 // transposed stage writes lambda_q and lambda_w to the partner buffers T1, T2 (inputs'
 // halos are read by neighbouring CTAs), the one-sided radial rows are added, the ghost
 // adjoints are scattered back, and the buffer pairs swap roles.
+template <typename T, int TX, int TY>
+static int launch_adj_stage(solar_ctx* c, AdjStageArgs<T>& a) {
+  using L = AdjLayout<T, TX, TY>;
+  AdjBuffers& b = c->adj;
+  if (!make_map(c, b.L, TX + 8, TY + 6, &a.mBq) || !make_map(c, b.LW, TX + 8, TY + 6, &a.mBw) ||
+      !make_map(c, b.L, TX, TY, &a.mTq) || !make_map(c, b.LW, TX, TY, &a.mTw))
+    return fail(SOLAR_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+  static bool attr_set = false;
+  if (!attr_set) {
+    CK(cudaFuncSetAttribute(adj_stage_kernel<T, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::TOTAL));
+    attr_set = true;
+  }
+  const Geom& g = c->g;
+  const long long tiles = 6LL * (g.n / TX) * (g.n / TY);
+  const long long want = 148LL * 6;
+  const int nch = (int)std::max<long long>(1, (want + tiles - 1) / tiles);
+  a.kchunk = std::max(8, (g.nr + nch - 1) / nch);
+  dim3 grid((unsigned)((g.n / TX) * (g.n / TY)), (unsigned)((g.nr + a.kchunk - 1) / a.kchunk), 6);
+  adj_stage_kernel<T, TX, TY><<<grid, TX * TY, L::TOTAL, c->stream>>>(a);
+  return SOLAR_OK;
+}
+
 template <typename T>
 static int enqueue_rhs_adjoint(solar_ctx* c, AdjStageArgs<T> a) {
   AdjBuffers& b = c->adj;
   const Geom& g = c->g;
-  a.lq = (const T*)b.L;
-  a.lw = (const T*)b.LW;
   a.lout = (T*)b.T1;
   a.lwout = (T*)b.T2;
   a.rb = (T*)b.rb;
-  const bool wide = g.n % 32 == 0;
-  const int tx = wide ? 32 : 16, ty = wide ? 8 : 16;
-  const long long tiles = 6LL * (g.n / tx) * (g.n / ty);
-  const long long want = 148LL * 6;
-  const int nch = (int)std::max<long long>(1, (want + tiles - 1) / tiles);
-  a.kchunk = std::max(8, (g.nr + nch - 1) / nch);
-  dim3 grid((unsigned)((g.n / tx) * (g.n / ty)), (unsigned)((g.nr + a.kchunk - 1) / a.kchunk), 6);
-  if (wide) adj_stage_kernel<T, 32, 8><<<grid, 256, 0, c->stream>>>(a);
-  else adj_stage_kernel<T, 16, 16><<<grid, 256, 0, c->stream>>>(a);
+  a.err = c->err;
+  if ((long long)g.nf * g.vs >= (1LL << 31))     // the kernel indexes one face's fields in 32 bits
+    return fail(SOLAR_ERR_ARG, "grid too large for the adjoint (%lld values per face)", (long long)g.nf * g.vs);
+  int rc = (g.n % 32 == 0) ? launch_adj_stage<T, 32, 8>(c, a) : launch_adj_stage<T, 16, 16>(c, a);
+  if (rc) return rc;
   adj_rbdy_kernel<T><<<blocks_for(6LL * 14 * g.n * g.n, 256), 256, 0, c->stream>>>((T*)b.T1, (const T*)b.rb,
                                                                                    (const T*)c->dt.rad, g, a.dt);
   adj_edge_kernel<T><<<dim3(blocks_for(g.n, 128), 72, g.nr), 128, 0, c->stream>>>(
