@@ -15,8 +15,8 @@
 //              transpose, on the interior and on the ghost frame -- the frame values are the
 //              adjoints of the neighbour faces' ghost values;
 //   adj_rbdy   the one-sided (Tam-Dong) rows of the radial transpose;
-//   adj_edge   the transpose of the edge exchange: ghost adjoints scattered (atomic adds)
-//              into the source faces' lines with the same folded coefficients.
+//   adj_edge   the transpose of the edge exchange: each source-line point gathers the ghost
+//              adjoints that used it, with the same folded coefficients.
 // FILTER_EXP^T is the radial transpose, then eta, then xi, each with its ghost-frame
 // adjoints, then the same scatter.
 #pragma once
@@ -366,53 +366,55 @@ __global__ void adj_rbdy_kernel(T* lout, const T* rb, const T* rad, Geom g, T dt
   lout[g.vol(0, face, g.slot[kVr]) + o] += dt * s2;
 }
 
-// Transpose of the edge exchange: every ghost-frame adjoint of buffer `q` is scattered back
-// onto the source lines of the neighbouring face.  mode 0: p scalar + the rotated vector
-// component (v_xi on W/E, v_eta on S/N); mode 1: every stored field scalar.
+// Transpose of the edge exchange, as a gather: every source-line point (the receiving face
+// and edge's route, layer l, position u along the source edge, plane k) sums the ghost
+// adjoints of the ghost points whose 9 taps include it -- a contiguous range of positions t,
+// tspan -- with the same folded coefficients, then adds the sum to its value (atomically:
+// the source lines of two edges of a face share their corner points).  mode 0: p scalar +
+// the rotated vector component (v_xi on W/E receivers, v_eta on S/N); mode 1: every stored
+// field scalar.  grid: x over u, y over (receiving face-edge, layer), z over planes.
 template <typename T>
 __global__ void adj_edge_kernel(T* q, const T* __restrict__ ew, const T* __restrict__ eg, const int* __restrict__ s0t,
-                                Geom g, int mode) {
-  // grid: x over positions t along the edge, y over (receiving face and edge, layer), z over planes
+                                const int* __restrict__ tspan, Geom g, int mode) {
   const int n = g.n;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
-  const int fe = blockIdx.y / 3, l = blockIdx.y % 3, k = blockIdx.z, run = 0;
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= n) return;
+  const int fe = blockIdx.y / 3, l = blockIdx.y % 3, k = blockIdx.z;
   const int face = fe >> 2, e = fe & 3;
   const EdgeRouteDev rt = cRoute[face][e];
   const bool along_i = rt.src_edge <= 1;
   const int fixed = (rt.src_edge == 0 || rt.src_edge == 2) ? l + 1 : n - 2 - l;
-  const int crow = (fe * 3 + l) * 9;
-  const int s0 = __ldg(s0t + (fe * 3 + l) * n + t);
-  long long dst;
-  if (e == 0) dst = g.at(k, -1 - l, t);
-  else if (e == 1) dst = g.at(k, n + l, t);
-  else if (e == 2) dst = g.at(k, t, -1 - l);
-  else dst = g.at(k, t, n + l);
-  auto src_at = [&](int s) {
-    const int ii = along_i ? s0 + s : fixed, jj = along_i ? fixed : s0 + s;
-    return g.at(k, jj, ii);
-  };
+  const int row = fe * 3 + l, crow = row * 9;
+  const int lo = __ldg(tspan + (row * n + u) * 2), hi = __ldg(tspan + (row * n + u) * 2 + 1);
+  if (hi < lo) return;
+  const long long src = g.at(k, along_i ? fixed : u, along_i ? u : fixed);
+  // receiver ghost position of (e, l, t): rows -1-l / n+l, columns -1-l / n+l
+  const long long g0 = (e == 0) ? g.at(k, -1 - l, 0) : (e == 1) ? g.at(k, n + l, 0)
+                     : (e == 2) ? g.at(k, 0, -1 - l) : g.at(k, 0, n + l);
+  const long long gstep = e <= 1 ? 1 : g.pitch;
+  const int* st = s0t + row * n;
   if (mode == 1) {
     for (int sl = 0; sl < g.nf; ++sl) {
-      const T gv = q[g.vol(run, face, sl) + dst];
-      T* dstv = q + g.vol(run, rt.src_face, sl);
-#pragma unroll
-      for (int s = 0; s < 9; ++s) atomicAdd(dstv + src_at(s), __ldg(ew + (crow + s) * n + t) * gv);
+      const T* gv = q + g.vol(0, face, sl) + g0;
+      T acc = T(0);
+      for (int t = lo; t <= hi; ++t) acc += __ldg(ew + (long long)(crow + u - __ldg(st + t)) * n + t) * gv[t * gstep];
+      atomicAdd(q + g.vol(0, rt.src_face, sl) + src, acc);
     }
     return;
   }
-  const T gp = q[g.vol(run, face, g.slot[kP]) + dst];
-  const T gv = q[g.vol(run, face, e >= 2 ? g.slot[kVxi] : g.slot[kVeta]) + dst];
-  T* pp = q + g.vol(run, rt.src_face, g.slot[kP]);
-  T* px = q + g.vol(run, rt.src_face, g.slot[kVxi]);
-  T* py = q + g.vol(run, rt.src_face, g.slot[kVeta]);
-#pragma unroll
-  for (int s = 0; s < 9; ++s) {
-    const long long o = src_at(s);
-    atomicAdd(pp + o, __ldg(ew + (crow + s) * n + t) * gp);
-    atomicAdd(px + o, __ldg(eg + ((crow + s) * 2 + 0) * n + t) * gv);
-    atomicAdd(py + o, __ldg(eg + ((crow + s) * 2 + 1) * n + t) * gv);
+  const T* gp = q + g.vol(0, face, g.slot[kP]) + g0;
+  const T* gvv = q + g.vol(0, face, e >= 2 ? g.slot[kVxi] : g.slot[kVeta]) + g0;
+  T ap = T(0), ax = T(0), ay = T(0);
+  for (int t = lo; t <= hi; ++t) {
+    const int r = crow + u - __ldg(st + t);
+    const T pv = gp[t * gstep], vv = gvv[t * gstep];
+    ap += __ldg(ew + (long long)r * n + t) * pv;
+    ax += __ldg(eg + ((long long)r * 2 + 0) * n + t) * vv;
+    ay += __ldg(eg + ((long long)r * 2 + 1) * n + t) * vv;
   }
+  atomicAdd(q + g.vol(0, rt.src_face, g.slot[kP]) + src, ap);
+  atomicAdd(q + g.vol(0, rt.src_face, g.slot[kVxi]) + src, ax);
+  atomicAdd(q + g.vol(0, rt.src_face, g.slot[kVeta]) + src, ay);
 }
 
 // FILTER_R^T for every stored field: u_m = sum over output planes k in [5, nr-6] of
@@ -444,33 +446,77 @@ __global__ void adj_filter_r_kernel(const T* lam, T* u, Geom g) {
   }
 }
 
-// FILTER_ETA^T (dir 1) or FILTER_XI^T (dir 0) with zero halos, evaluated on the interior and
-// on the ghost rows (eta) / columns (xi) of the face.  Interior results go to `out`'s
-// interior; ghost results are the adjoints of the (unfiltered) halo values and go to
-// `frame`'s frame.
-template <typename T>
-__global__ void adj_filter_dir_kernel(const T* __restrict__ in, T* out, T* frame, Geom g, int dir) {
-  // grid: x over the points of a row (n + 6 extended columns for xi, n for eta), y over rows
-  // (n for xi, n + 6 extended rows for eta), z over (field volume, plane)
+// FILTER_XI^T (FILTER_ETA^T (u)) for one TX x TY tile of one plane of one field volume: the
+// transposes of the two in-face filters of FILTER_EXP with zero halos.  u (the adjoint of
+// the eta filter's output) lives on the face interior only.  v = FILTER_ETA^T u is formed in
+// shared memory on the tile rows and xi-halo columns; on S/N edge tiles v on the three ghost
+// rows is the adjoint of the eta filter's (unfiltered) halo and goes to the frame.  The
+// interior output is FILTER_XI^T v; on W/E edge tiles the xi filter's halo adjoints go to
+// the ghost columns.
+template <typename T, int TX, int TY, int KP>
+__global__ void __launch_bounds__(TX * TY) adj_filter_xy_kernel(const T* __restrict__ in, T* out, Geom g) {
+  constexpr int BW = TX + 6, BH = TY + 6, NB = BW * BH, NT = TX * TY, PER = (NB + NT - 1) / NT;
+  __shared__ T su[BH][BW], sv[BH][BW];
   const int n = g.n;
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y;
-  if (x >= (dir ? n : n + 6)) return;
-  const int k = blockIdx.z % g.nr;
-  const long long vbase = (long long)(blockIdx.z / g.nr) * g.vs;
-  const int a_ = dir ? y - 3 : x - 3;                     // along the filter direction
-  const int b_ = dir ? x : y;                             // the other in-face coordinate
-  const T* f = in + vbase;
-  auto val = [&](int aa) -> T {
-    if (aa < 0 || aa >= n) return T(0);
-    return __ldg(dir ? f + g.at(k, aa, b_) : f + g.at(k, b_, aa));
-  };
-  T s = Coef<T>::filt(0) * val(a_);
+  const int tiles_x = n / TX;
+  const int i0 = (blockIdx.x % tiles_x) * TX, j0 = (blockIdx.x / tiles_x) * TY;
+  const int k0 = blockIdx.y * KP, k1 = min(g.nr, k0 + KP);
+  const long long vbase = (long long)blockIdx.z * g.vs;              // field volume
+  const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
+  const T f0 = Coef<T>::filt(0), f1 = Coef<T>::filt(1), f2 = Coef<T>::filt(2), f3 = Coef<T>::filt(3);
+  // this thread's box entries and their in-plane offsets (-1: outside the face)
+  int boff[PER];
 #pragma unroll
-  for (int m = 1; m <= 3; ++m) s += Coef<T>::filt(m) * (val(a_ - m) + val(a_ + m));
-  const long long pt = dir ? g.at(k, a_, b_) : g.at(k, b_, a_);
-  if (a_ >= 0 && a_ < n) out[vbase + pt] = s;
-  else frame[vbase + pt] = s;
+  for (int e = 0; e < PER; ++e) {
+    const int q = tid + e * NT;
+    const int br = q / BW, bc = q % BW;
+    const int gj = j0 - 3 + br, gi = i0 - 3 + bc;
+    boff[e] = (q < NB && gi >= 0 && gi < n && gj >= 0 && gj < n) ? (JOFF + gj) * g.pitch + IOFF + gi : -1;
+  }
+  T nxt[PER];
+  auto fetch = [&](int k) {
+    const T* u = in + vbase + (long long)k * g.plane;
+#pragma unroll
+    for (int e = 0; e < PER; ++e) nxt[e] = boff[e] >= 0 ? u[boff[e]] : T(0);
+  };
+  if (k0 < k1) fetch(k0);
+  auto U = [&](int br, int bc) { return (br >= 0 && br < BH) ? su[br][bc] : T(0); };
+  auto Vv = [&](int br, int bc) { return (bc >= 0 && bc < BW) ? sv[br][bc] : T(0); };
+  auto xt = [&](int br, int bc) {
+    return f0 * Vv(br, bc) + f1 * (Vv(br, bc - 1) + Vv(br, bc + 1)) + f2 * (Vv(br, bc - 2) + Vv(br, bc + 2)) +
+           f3 * (Vv(br, bc - 3) + Vv(br, bc + 3));
+  };
+  for (int k = k0; k < k1; ++k) {
+#pragma unroll
+    for (int e = 0; e < PER; ++e) {
+      const int q = tid + e * NT;
+      if (q < NB) su[q / BW][q % BW] = nxt[e];
+    }
+    __syncthreads();
+    if (k + 1 < k1) fetch(k + 1);                                    // next plane in flight
+    for (int q = tid; q < NB; q += NT) {
+      const int br = q / BW, bc = q % BW;
+      sv[br][bc] = f0 * U(br, bc) + f1 * (U(br - 1, bc) + U(br + 1, bc)) + f2 * (U(br - 2, bc) + U(br + 2, bc)) +
+                   f3 * (U(br - 3, bc) + U(br + 3, bc));
+    }
+    __syncthreads();
+    T* o = out + vbase + (long long)k * g.plane;
+    const int j = j0 + ty, i = i0 + tx;
+    o[(JOFF + j) * g.pitch + IOFF + i] = xt(ty + 3, tx + 3);
+    // eta-filter halo adjoints: v on the ghost rows (interior columns)
+    if (tid < 3 * TX && (j0 == 0 || j0 + TY == n)) {
+      const int r = tid / TX, c = tid % TX;
+      if (j0 == 0) o[(JOFF - 3 + r) * g.pitch + IOFF + i0 + c] = sv[r][c + 3];
+      if (j0 + TY == n) o[(JOFF + n + r) * g.pitch + IOFF + i0 + c] = sv[TY + 3 + r][c + 3];
+    }
+    // xi-filter halo adjoints on the ghost columns (interior rows)
+    if (tid < 3 * TY && (i0 == 0 || i0 + TX == n)) {
+      const int c = tid / TY, r = tid % TY;
+      if (i0 == 0) o[(JOFF + j0 + r) * g.pitch + IOFF - 3 + c] = xt(r + 3, c);
+      if (i0 + TX == n) o[(JOFF + j0 + r) * g.pitch + IOFF + n + c] = xt(r + 3, TX + 3 + c);
+    }
+    __syncthreads();                                                 // su/sv reused next plane
+  }
 }
 
 // Receivers: p sampled with trilinear weights over the 8 grid points around each receiver

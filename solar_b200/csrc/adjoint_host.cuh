@@ -23,6 +23,8 @@ static int adj_alloc(solar_ctx* c) {
   }
   CK(cudaMalloc((void**)&b.grad, (size_t)6 * vol_compact(c) * sizeof(double)));
   CK(cudaMalloc(&b.rb, (size_t)6 * 4 * 2 * c->g.n * c->g.n * c->esize));
+  CK(cudaMalloc((void**)&b.tspan, c->ht.tspan.size() * sizeof(int)));
+  CK(cudaMemcpy(b.tspan, c->ht.tspan.data(), c->ht.tspan.size() * sizeof(int), cudaMemcpyHostToDevice));
   return SOLAR_OK;
 }
 
@@ -105,7 +107,7 @@ static int enqueue_rhs_adjoint(solar_ctx* c, AdjStageArgs<T> a) {
   adj_rbdy_kernel<T><<<blocks_for(6LL * 14 * g.n * g.n, 256), 256, 0, c->stream>>>((T*)b.T1, (const T*)b.rb,
                                                                                    (const T*)c->dt.rad, g, a.dt);
   adj_edge_kernel<T><<<dim3(blocks_for(g.n, 128), 72, g.nr), 128, 0, c->stream>>>(
-      (T*)b.T1, (const T*)c->dt.ew, (const T*)c->dt.eg, c->dt.s0t, g, 0);
+      (T*)b.T1, (const T*)c->dt.ew, (const T*)c->dt.eg, c->dt.s0t, b.tspan, g, 0);
   CK(cudaGetLastError());
   std::swap(b.L, b.T1);
   std::swap(b.LW, b.T2);
@@ -118,13 +120,15 @@ static int enqueue_filter_adjoint(solar_ctx* c) {
   const Geom& g = c->g;
   T* L = (T*)c->adj.L;
   T* T1 = (T*)c->adj.T1;
-  T* T2 = (T*)c->adj.T2;
   adj_filter_r_kernel<T><<<blocks_for(6LL * g.nf * g.n * g.n, 128), 128, 0, c->stream>>>(L, T1, g);
-  const unsigned zvol = (unsigned)(6 * g.nf * g.nr);
-  adj_filter_dir_kernel<T><<<dim3(blocks_for(g.n, 128), g.n + 6, zvol), 128, 0, c->stream>>>(T1, T2, L, g, 1);
-  adj_filter_dir_kernel<T><<<dim3(blocks_for(g.n + 6, 128), g.n, zvol), 128, 0, c->stream>>>(T2, L, L, g, 0);
+  constexpr int KP = 8;                                             // planes per CTA
+  const unsigned kch = (unsigned)((g.nr + KP - 1) / KP);
+  if (g.n % 32 == 0)
+    adj_filter_xy_kernel<T, 32, 8, KP><<<dim3((g.n / 32) * (g.n / 8), kch, 6 * g.nf), 256, 0, c->stream>>>(T1, L, g);
+  else
+    adj_filter_xy_kernel<T, 16, 16, KP><<<dim3((g.n / 16) * (g.n / 16), kch, 6 * g.nf), 256, 0, c->stream>>>(T1, L, g);
   adj_edge_kernel<T><<<dim3(blocks_for(g.n, 128), 72, g.nr), 128, 0, c->stream>>>(
-      L, (const T*)c->dt.ew, (const T*)c->dt.eg, c->dt.s0t, g, 1);
+      L, (const T*)c->dt.ew, (const T*)c->dt.eg, c->dt.s0t, c->adj.tspan, g, 1);
   CK(cudaGetLastError());
   return SOLAR_OK;
 }

@@ -352,6 +352,18 @@ int build_tables(const solar_desc& d, HostTables& t, std::string& err) {
         }
       }
     }
+  t.tspan.assign((size_t)6 * 4 * 3 * n * 2, 0);
+  for (size_t fl = 0; fl < (size_t)6 * 4 * 3; ++fl)
+    for (int u = 0; u < n; ++u) {
+      int lo = n, hi = -1;
+      for (int q = 0; q < n; ++q) {
+        const int s0 = t.s0t[fl * n + q];
+        if (u >= s0 && u <= s0 + 8) { lo = std::min(lo, q); hi = std::max(hi, q); }
+      }
+      if (hi < 0) lo = 0;
+      t.tspan[(fl * n + u) * 2 + 0] = lo;
+      t.tspan[(fl * n + u) * 2 + 1] = hi;
+    }
   return SOLAR_OK;
 }
 

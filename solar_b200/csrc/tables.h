@@ -82,6 +82,9 @@ struct HostTables {
   std::vector<double> ew;                          // [6][4][3][9][n]
   std::vector<double> eg;                          // [6][4][3][9][2][n]
   std::vector<int> s0t;                            // [6][4][3][n]
+  // Transposed exchange: the ghost points t whose 9 taps include source position u form a
+  // contiguous range, tspan[f][e][l][u] = (first t, last t); (0, -1) when empty.
+  std::vector<int> tspan;                          // [6][4][3][n][2]
   // COMPUTE_CURL's vector halos carry both receiver components:
   //   ghost_out = sum_s egc[f][e][l][s][out][in][t] * v_in(tap s),  out/in = (xi, eta)
   std::vector<double> egc;                         // [6][4][3][9][2][2][n]
