@@ -318,7 +318,8 @@ def split_block(cfg, args, world, local):
 
     from solar_b200 import distributed as D
 
-    if not dist.is_initialized():             # one process: a one-rank group
+    own_group = not dist.is_initialized()
+    if own_group:                             # one process: a one-rank group
         import socket
         with socket.socket() as sk:
             sk.bind(("127.0.0.1", 0))
@@ -336,6 +337,8 @@ def split_block(cfg, args, world, local):
     ms = max_over_ranks(e0.elapsed_time(e1), world)
     norm = zs.norm(4)
     zs.close()
+    if own_group:
+        dist.destroy_process_group()
     return {"value": cfg.points * args.steps / (ms / 1e3), "unit": "grid-pt RK4 updates/s", "scaling": "strong",
             "ms_per_step": ms / args.steps, "zones_per_rank": 6 // world, "norm_vr": norm}
 
