@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const __grid_cons
       const T hc2 = (do_halo && a.c2) ? __ldg(a.c2 + plane_c2 + hq2) : T(0);
       const T invr = __ldg(rad + rInvR * nr + m), inv_rho0 = __ldg(rad + rInvRho0 * nr + m);
       const T rho0 = __ldg(rad + rRho0 * nr + m), c2r = __ldg(rad + rC2Rho0 * nr + m);
-      ok &= mbar_wait(&bars[slot], phase, a.err, 5);
+      ok &= mbar_wait(&bars[slot], phase, a.err, kErrAdjointRing);
       const T* sb = reinterpret_cast<const T*>(slot_base(slot));
       constexpr int PBs = (int)(L::P_BYTES / sizeof(T)), OBs = (int)(L::O_BYTES / sizeof(T));
       T lqv[5], lwv[5];

@@ -52,7 +52,7 @@ __global__ void force_clock_kernel(ForceClock* c, int kind, double diml, double 
       c->den[m] = p;
       bool on = m >= 4 ? (m == 4 || (m == 5 && fl < nstep) || (m == 6 && fl < nstep - 1)) : c->x[m] >= 0.0;
       int s = fl - 4 + m;                        // S_t(:,:,floor(xt)-3+m), 1-based
-      if (on && (s < 0 || s >= nt)) { on = false; atomicExch(err, 2); }
+      if (on && (s < 0 || s >= nt)) { on = false; atomicExch(err, kErrForcingSample); }
       c->idx[m] = on ? s : -1;
     }
     c->step_old = fl;

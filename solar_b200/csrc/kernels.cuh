@@ -115,168 +115,242 @@ __device__ __forceinline__ void stv(T* p, const T* in) {
 // mode 1: filter halos -- every stored field, scalar, all edges (filter.f90:23-28).
 template <typename T>
 struct EdgeArgs {
+  CUtensorMap mRow;         // tiles {sp, 3 rows} of the buffer (source lines along i)
+  CUtensorMap mCol;         // tiles {4, sp rows} of the buffer (source lines along j)
   T* q;                     // buffer whose frames are filled (its interior is the source)
   const T* ew;              // [6][4][3][9][n]     scalar tap weights, position fastest
   const T* eg;              // [6][4][3][9][2][n]  vector tap weights (v_xi, v_eta)
   const int* s0t;           // [6][4][3][n]        first tap along the source edge
   const int* active;        // per-run flag or nullptr
+  const int2* win;          // [24][nseg] staged source window (first position, count)
   Geom g;
   int mode;
-  int kchunk;
+  int kchunk;               // planes per CTA
+  int ts, nseg;             // positions per segment, segments per edge
+  int ngroups;              // field groups per edge: 2 in mode 0, ceil(nf / 2) in mode 1
+  int sp;                   // staged positions per line (window capacity, a multiple of 8)
+  int* err;                 // device error word (a bounded wait gave up)
 };
 
-// One CTA per (run, receiving face and edge, chunk of up to KC planes).  The source face's
-// three edge lines of every needed field are staged in shared memory with asynchronous
-// copies (rows as 16-byte pieces, columns three values per row), then each thread
-// produces the ghost values of its (position, layer) pairs for all staged planes at
-// once, so the planes' tap sums run in parallel.  Coefficient tables are stored
-// position-fastest ([face][edge][layer][tap][position]) so every table load of a warp is
-// one contiguous segment.
-// Resident CTAs per SM the compiler budgets registers for: the kernel is latency-bound,
-// so float with at most 2 planes per CTA is held to 64 registers (measured faster); double
-// and 4-plane float keep their registers (a tighter budget spills).
-template <typename T, int KC> struct EdgeMinBlocks { static constexpr int value = (sizeof(T) == 4 && KC <= 2) ? 8 : 1; };
+// One CTA per (run, receiving face and edge, field group, segment of ts positions along
+// the edge, chunk of planes).  Field groups: mode 0 -> {p} and {v_xi, v_eta} (one rotated
+// output); mode 1 -> pairs of stored fields, each scalar.  Each of the 3 * ts threads owns
+// one (layer, position) ghost point and keeps its 9 (scalar) or 18 (vector) tap weights in
+// registers for the whole chunk, while the CTA marches the planes through kEdgeRing staging
+// slots that thread 0 fills with TMA tile loads kEdgeDepth planes ahead of the plane being
+// computed (one mbarrier per slot):
+//   source lines along i (S/N source edges): box {sp, 3 rows} per field -> [row][u];
+//   source lines along j (W/E): the three columns of a row lie in one aligned 4-value
+//     group; box {4, sp rows} per field -> [u][4], spread to [layer][u] one plane before
+//     use (tap reads from the 4-value groups would be 4-way bank conflicts).
+// A tile load is one request for the whole strided box, so a plane's 3 x sp source values
+// cost the SM no per-row load instructions and no per-row miss tracking.
+// S/N receivers store their ghost rows directly.  W/E receivers park a plane's results in
+// shared memory and one thread per row writes the row's whole 32-byte sector (ghost
+// columns plus the padding next to them): writing 12 of 32 bytes would make the L2 read
+// the sector back from DRAM to merge it.
+constexpr int kEdgeDepth = 6;               // planes in flight ahead of the computed one
+constexpr int kEdgeRing = kEdgeDepth + 2;   // a slot is refilled two planes after its last read
 
-template <typename T, int KC>
-__global__ void __launch_bounds__(128, (EdgeMinBlocks<T, KC>::value)) edge_kernel(const EdgeArgs<T> a) {
-  extern __shared__ __align__(16) unsigned char esm[];
-  T* buf = reinterpret_cast<T*>(esm);                    // [field][kk][layer][t_s]
+// Shared memory of one CTA in bytes: staging ring (two fields of 4 * sp values per slot),
+// spread planes, parked W/E results, one mbarrier per slot.
+__host__ __device__ inline int edge_smem_bytes(int sp, int ts, int esize) {
+  return (kEdgeRing * 8 * sp + 16 * sp + 12 * ts) * esize + kEdgeRing * 8;
+}
+
+// Resident CTAs per SM the registers are budgeted for (3 x 384 threads in float).
+template <typename T> struct EdgeMinBlocks { static constexpr int value = sizeof(T) == 4 ? 3 : 2; };
+
+template <typename T>
+__global__ void __launch_bounds__(384, (EdgeMinBlocks<T>::value)) edge_kernel(const __grid_constant__ EdgeArgs<T> a) {
+  extern __shared__ __align__(128) unsigned char esm[];
   const Geom& g = a.g;
-  const int n = g.n;
-  const int fe = g.face0 * 4 + blockIdx.y, face = fe >> 2, e = fe & 3, run = blockIdx.z;
+  const int n = g.n, ts = a.ts, sp = a.sp;
+  const int run = blockIdx.z;
   if (a.active && !a.active[run]) return;
-  const int kb = blockIdx.x * KC;
+  const int kb = blockIdx.x * a.kchunk;
   if (kb >= g.nr) return;
-  const int kc = min(KC, g.nr - kb);
+  const int kc = min(a.kchunk, g.nr - kb);
+  int y = blockIdx.y;
+  const int seg = y % a.nseg;
+  y /= a.nseg;
+  const int grp = y % a.ngroups;
+  const int fe = g.face0 * 4 + y / a.ngroups, face = fe >> 2, e = fe & 3;
   const EdgeRouteDev rt = cRoute[face][e];
   const bool along_i = rt.src_edge <= 1;                 // S/N source lines run along i
   const bool low = (rt.src_edge == 0 || rt.src_edge == 2);
-  const int nfl = a.mode == 1 ? g.nf : 3;                // staged fields
-  auto slot_of = [&](int f) {
-    return a.mode == 1 ? f : (f == 0 ? g.slot[kP] : (f == 1 ? g.slot[kVxi] : g.slot[kVeta]));
-  };
-  for (int fk = 0; fk < nfl * kc; ++fk) {               // uniform over the CTA
-    const int f = fk / kc, kk = fk - f * kc;
-    const T* src = a.q + g.vol(run, rt.src_face, slot_of(f)) + (long long)(kb + kk) * g.plane;
-    T* dst = buf + (long long)(f * KC + kk) * 3 * n;
-    if (along_i) {                                       // rows: 16-byte pieces
-      constexpr int W16 = 16 / sizeof(T);
-      for (int idx = threadIdx.x * W16; idx < 3 * n; idx += blockDim.x * W16) {
-        const int l = idx / n, t = idx - l * n;
-        const T* rowp = src + (long long)(JOFF + (low ? l + 1 : n - 2 - l)) * g.pitch + IOFF;
-        cp_async_16(dst + idx, rowp + t);
-      }
-    }
+  const bool cols = e >= 2;                              // W/E receiver: ghost columns
+  const bool vec = a.mode != 1 && grp == 1;              // {v_xi, v_eta} -> one rotated component
+  int nsrc, nout, sl0, sl1, ol0, ol1;
+  if (a.mode == 1) {
+    sl0 = ol0 = 2 * grp;
+    sl1 = ol1 = min(2 * grp + 1, g.nf - 1);
+    nsrc = nout = min(2, g.nf - 2 * grp);
+  } else if (!vec) {
+    sl0 = sl1 = ol0 = ol1 = g.slot[kP];
+    nsrc = nout = 1;
+  } else {
+    sl0 = g.slot[kVxi];
+    sl1 = g.slot[kVeta];
+    ol0 = ol1 = cols ? g.slot[kVxi] : g.slot[kVeta];
+    nsrc = 2;
+    nout = 1;
   }
-  if (!along_i) {
-    // columns: the three layers of a row lie in one aligned 4-value group (columns 0..3 or
-    // n-4..n-1), fetched as 16-byte vectors and spread to the [layer][t] layout
-    const int c0 = low ? 0 : n - 4;
-    constexpr int W16 = 16 / sizeof(T);
-#pragma unroll 4
-    for (int idx = threadIdx.x; idx < nfl * kc * n; idx += blockDim.x) {
-      const int fk = idx / n, t = idx - fk * n;
-      const int f = fk / kc, kk = fk - f * kc;
-      const T* rp = a.q + g.vol(run, rt.src_face, slot_of(f)) + (long long)(kb + kk) * g.plane +
-                    (long long)(JOFF + t) * g.pitch + IOFF + c0;
-      T v[4];
-      ldv(rp, v);
-      if (W16 == 2) ldv(rp + 2, v + 2);
-      T* dst = buf + (long long)(f * KC + kk) * 3 * n;
-#pragma unroll
-      for (int l = 0; l < 3; ++l) dst[l * n + t] = v[low ? 1 + l : 2 - l];
-    }
-  }
-  cp_async_wait_all();
-  __syncthreads();
-  const long long fstr = (long long)KC * 3 * n;         // field stride inside buf
-  // W/E receivers write their three ghost columns of a row as one whole 32-byte sector
-  // (ghost layers plus the unused padding columns next to them); writing 12 of 32 bytes
-  // would make the L2 read the sector back from DRAM to merge it.
-  const bool cols = e >= 2;
+  const int lo = a.win[fe * a.nseg + seg].x;             // first staged source position
+  const int tid = threadIdx.x;
+  const int l = tid / ts, tl = tid - l * ts, t = seg * ts + tl;
+  const bool valid = t < n;
   constexpr int SECT = 32 / sizeof(T);                   // elements per 32-byte sector
-  const int npairs = cols ? n : 3 * n;
-  for (int pr = threadIdx.x; pr < npairs; pr += blockDim.x) {
-    const int t = cols ? pr : pr % n;
-    const int lfirst = cols ? 0 : pr / n, lcount = cols ? 3 : 1;
-    // write the planes of one field: rows for S/N receivers, one sector per row for W/E
-    auto put = [&](T* base, const T (&res)[3][KC]) {
+  const int FS = 4 * sp;                                 // field stride inside a slot / spread plane
+  const int SLOT = 2 * FS;
+  T* const sm = reinterpret_cast<T*>(esm);
+  T* const tb = sm + kEdgeRing * SLOT;                   // [2][2 fields][4 sp]: [layer][u] planes
+  T* const res = tb + 4 * FS;                            // [2][2 outputs][3 layers][ts]
+  uint64_t* const bars = reinterpret_cast<uint64_t*>(res + 12 * ts);
+
+  // tap weights and window offset of this thread's ghost point
+  T c0[9], c1[9];
+  const int s0 = valid ? a.s0t[((long long)fe * 3 + l) * n + t] - lo : 0;   // idle threads read the window start
+  {
+    const int tc = valid ? t : 0;
+    const long long crow = ((long long)fe * 3 + l) * 9;
 #pragma unroll
-      for (int kk = 0; kk < KC; ++kk) {
-        if (kk >= kc) continue;
-        if (!cols) {
-          base[(long long)kk * g.plane + g.at(0, e == 0 ? -1 - lfirst : n + lfirst, t)] = res[0][kk];
-        } else {
-          T sect[SECT];
-#pragma unroll
-          for (int m = 0; m < SECT; ++m) sect[m] = T(0);
-#pragma unroll
-          for (int l = 0; l < 3; ++l) sect[e == 2 ? SECT - 1 - l : l] = res[l][kk];
-          T* d = base + (long long)kk * g.plane + g.at(0, t, e == 2 ? -SECT : n);
-          stv(d, sect);
-          stv(d + Vec16<T>::V, sect + Vec16<T>::V);
-        }
+    for (int s = 0; s < 9; ++s) {
+      if (vec) {
+        c0[s] = a.eg[((crow + s) * 2 + 0) * n + tc];
+        c1[s] = a.eg[((crow + s) * 2 + 1) * n + tc];
+      } else {
+        c0[s] = a.ew[(crow + s) * n + tc];
+        c1[s] = T(0);
       }
-    };
-    if (a.mode == 1) {
-      for (int f = 0; f < nfl; ++f) {
-        T res[3][KC];
-        for (int li = 0; li < lcount; ++li) {
-          const int l = lfirst + li;
-          const long long crow = ((long long)fe * 3 + l) * 9;
-          const T* b0 = buf + f * fstr + l * n + a.s0t[((long long)fe * 3 + l) * n + t];
-          T w[9];
-#pragma unroll
-          for (int s = 0; s < 9; ++s) w[s] = a.ew[(crow + s) * n + t];
-#pragma unroll
-          for (int kk = 0; kk < KC; ++kk) {
-            const T* b = b0 + kk * 3 * n;
-            T a0 = T(0), a1 = T(0);
-            if (kk < kc) {
-#pragma unroll
-              for (int s = 0; s < 9; s += 2) a0 = fma(w[s], b[s], a0);
-#pragma unroll
-              for (int s = 1; s < 9; s += 2) a1 = fma(w[s], b[s], a1);
-            }
-            res[li][kk] = a0 + a1;
-          }
-        }
-        put(a.q + g.vol(run, face, slot_of(f)) + (long long)kb * g.plane, res);
-      }
-      continue;
     }
-    T res_p[3][KC], res_v[3][KC];
-    for (int li = 0; li < lcount; ++li) {
-      const int l = lfirst + li;
-      const long long crow = ((long long)fe * 3 + l) * 9;
-      const int b0 = l * n + a.s0t[((long long)fe * 3 + l) * n + t];
-      T w[9], gx[9], gy[9];
+  }
+  // tile coordinates of the chunk's first plane (z counts planes over run, face, field, k)
+  const int zs0 = ((run * 6 + rt.src_face) * g.nf + sl0) * g.nr + kb;
+  const int zs1 = ((run * 6 + rt.src_face) * g.nf + sl1) * g.nr + kb;
+  const int tx = along_i ? IOFF + lo : IOFF + (low ? 0 : n - 4);
+  const int ty = along_i ? JOFF + (low ? 1 : n - 4) : JOFF + lo;
+  const uint32_t tbytes = (uint32_t)(nsrc * (along_i ? 3 : 4) * sp * sizeof(T));
+  auto issue = [&](int kk, int slot) {                   // thread 0: both fields of plane kk
+    uint64_t* bar = bars + slot;
+    mbar_expect_tx(bar, tbytes);
+    const CUtensorMap* m = along_i ? &a.mRow : &a.mCol;
+    tma_load_3d(sm + slot * SLOT, m, tx, ty, zs0 + kk, bar);
+    if (nsrc == 2) tma_load_3d(sm + slot * SLOT + FS, m, tx, ty, zs1 + kk, bar);
+  };
+
+  // spread piece (column sources): one row of one field per thread
+  const bool spreader = !along_i && tid < nsrc * sp;
+  const int spf = tid >= sp ? 1 : 0, spu = tid - spf * sp;
+  const int sp_src = spf * FS + spu * 4, sp_dst = spf * FS + spu;
+  // outputs: S/N receivers store rows directly; W/E receivers write sectors from `res`
+  T* const dst0 = a.q + g.vol(run, face, ol0) + (long long)kb * g.plane;
+  T* const dst1 = a.q + g.vol(run, face, ol1) + (long long)kb * g.plane;
+  T* gout0 = dst0 + g.at(0, e == 0 ? -1 - l : n + l, valid ? t : 0);
+  const long long gap = dst1 - dst0;                     // second output field
+  const bool writer = cols && tid < ts && seg * ts + tid < n;
+  T* sec0 = dst0 + g.at(0, writer ? seg * ts + tid : 0, e == 2 ? -SECT : n);
+  // tap window inside a [layer][u] plane; row sources hold the layers in row order
+  const int boff = (along_i && !low ? 2 - l : l) * sp + s0;
+
+  auto spread = [&](int slot, int half) {                // [f][u][4] -> [f][layer][u]
+    if (spreader) {
+      T v[4];
+      ldv(sm + slot * SLOT + sp_src, v);
+      if (sizeof(T) == 8) ldv(sm + slot * SLOT + sp_src + 2, v + 2);
+      T* d = tb + half * 2 * FS + sp_dst;
+#pragma unroll
+      for (int ll = 0; ll < 3; ++ll) d[ll * sp] = v[low ? 1 + ll : 2 - ll];
+    }
+  };
+  auto put_sector = [&](T* d, const T* r) {
+    T sect[SECT];
+#pragma unroll
+    for (int m = 0; m < SECT; ++m) sect[m] = T(0);
+    if (e == 2) {
+#pragma unroll
+      for (int ll = 0; ll < 3; ++ll) sect[SECT - 1 - ll] = r[ll * ts];
+    } else {
+#pragma unroll
+      for (int ll = 0; ll < 3; ++ll) sect[ll] = r[ll * ts];
+    }
+    stv(d, sect);
+    stv(d + Vec16<T>::V, sect + Vec16<T>::V);
+  };
+  auto sectors = [&](int half) {                         // W/E: one whole sector per row
+    if (writer) {
+      const T* r = res + half * 6 * ts + tid;
+      put_sector(sec0, r);
+      if (nout == 2) put_sector(sec0 + gap, r + 3 * ts);
+      sec0 += g.plane;
+    }
+  };
+
+  if (tid == 0) {
+    for (int s = 0; s < kEdgeRing; ++s) mbar_init(bars + s, 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  if (tid == 0)
+    for (int d = 0; d < kEdgeDepth && d < kc; ++d) issue(d, d);
+  mbar_wait(bars, 0, a.err, kErrEdgeRing);
+  spread(0, 0);
+  int rs = 0;                                            // ring slot of plane kk
+  int ws = kEdgeDepth;                                   // ring slot of plane kk + kEdgeDepth
+  int ns = 1;                                            // ring slot of plane kk + 1 ...
+  uint32_t np = 0;                                       // ... and the parity of its phase
+  for (int kk = 0; kk < kc; ++kk) {
+    if (tid == 0 && kk + kEdgeDepth < kc) issue(kk + kEdgeDepth, ws);
+    ws = ws + 1 == kEdgeRing ? 0 : ws + 1;
+    if (ns == 0) np ^= 1;
+    if (kk + 1 < kc) mbar_wait(bars + ns, np, a.err, kErrEdgeRing);
+    __syncthreads();
+    if (kk > 0) sectors((kk - 1) & 1);
+    if (kk + 1 < kc) spread(ns, (kk + 1) & 1);
+    const T* b = (along_i ? sm + rs * SLOT : tb + (kk & 1) * 2 * FS) + boff;
+    T r0, r1 = T(0);
+    if (vec) {
+      T a0 = T(0), a1 = T(0);
 #pragma unroll
       for (int s = 0; s < 9; ++s) {
-        w[s] = a.ew[(crow + s) * n + t];
-        gx[s] = a.eg[((crow + s) * 2 + 0) * n + t];
-        gy[s] = a.eg[((crow + s) * 2 + 1) * n + t];
+        a0 = fma(c0[s], b[s], a0);
+        a1 = fma(c1[s], b[FS + s], a1);
       }
+      r0 = a0 + a1;
+    } else {
+      T a0 = T(0), a1 = T(0);
 #pragma unroll
-      for (int kk = 0; kk < KC; ++kk) {
-        T ap = T(0), ax = T(0), ay = T(0);
-        if (kk < kc) {
-          const T* bp = buf + b0 + kk * 3 * n;
-          const T* bx = bp + fstr;
-          const T* by = bx + fstr;
+      for (int s = 0; s < 9; s += 2) a0 = fma(c0[s], b[s], a0);
 #pragma unroll
-          for (int s = 0; s < 9; ++s) {
-            ap = fma(w[s], bp[s], ap);
-            ax = fma(gx[s], bx[s], ax);
-            ay = fma(gy[s], by[s], ay);
-          }
-        }
-        res_p[li][kk] = ap;
-        res_v[li][kk] = ax + ay;
+      for (int s = 1; s < 9; s += 2) a1 = fma(c0[s], b[s], a1);
+      r0 = a0 + a1;
+      if (nout == 2) {
+        const T* b1 = b + FS;
+        T a2 = T(0), a3 = T(0);
+#pragma unroll
+        for (int s = 0; s < 9; s += 2) a2 = fma(c0[s], b1[s], a2);
+#pragma unroll
+        for (int s = 1; s < 9; s += 2) a3 = fma(c0[s], b1[s], a3);
+        r1 = a2 + a3;
       }
     }
-    put(a.q + g.vol(run, face, g.slot[kP]) + (long long)kb * g.plane, res_p);
-    put(a.q + g.vol(run, face, cols ? g.slot[kVxi] : g.slot[kVeta]) + (long long)kb * g.plane, res_v);
+    if (!cols) {
+      if (valid) {
+        *gout0 = r0;
+        if (nout == 2) gout0[gap] = r1;
+      }
+      gout0 += g.plane;
+    } else {
+      T* rr = res + (kk & 1) * 6 * ts + l * ts + tl;
+      rr[0] = r0;
+      rr[3 * ts] = r1;
+    }
+    rs = ns;
+    ns = ns + 1 == kEdgeRing ? 0 : ns + 1;
+  }
+  if (cols) {
+    __syncthreads();
+    sectors((kc - 1) & 1);
   }
 }
 
@@ -478,7 +552,7 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __
   for (int k = kb; k < ke; ++k) {
     const int ks = clampk(k);
     for (; mq <= ks + 6; ++mq) {
-      ok &= mbar_wait(&barL[slot_q], phase_q, a.err, 1);
+      ok &= mbar_wait(&barL[slot_q], phase_q, a.err, kErrStageLead);
       const T* bp = reinterpret_cast<const T*>(lead(slot_q));
 #pragma unroll
       for (int s = 0; s < 6; ++s)
@@ -488,7 +562,7 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __
       ldv(reinterpret_cast<const T*>(lead(slot_q) + L::P_BYTES) + oc, vw[6]);
       if (++slot_q == kLead) { slot_q = 0; phase_q ^= 1; }
     }
-    ok &= mbar_wait(&barT[slot_t], phase_t, a.err, 2);
+    ok &= mbar_wait(&barT[slot_t], phase_t, a.err, kErrStageTile);
     const Rad rn = load_rad(min(k + 1, nr - 1));
     const T* sp = reinterpret_cast<const T*>(lead(slot_k));
     const unsigned char* tb = tile(slot_t);
@@ -709,7 +783,7 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) filter_kernel(const _
     for (int u = 0; u < 11; ++u) {
       const int k = kb + u;
       if (k >= nr) break;
-      ok &= mbar_wait(&bars[slot], phase, a.err, 3);
+      ok &= mbar_wait(&bars[slot], phase, a.err, kErrFilterRing);
       const T* bx = reinterpret_cast<const T*>(smem + slot * L::P_BYTES);
       T* t1 = reinterpret_cast<T*>(smem + kFiltRing * L::P_BYTES + (k & 1) * L::S_BYTES);
       // xi filter of the box rows (columns V*cx .. V*cx+V-1 of the tile)

@@ -47,6 +47,8 @@ struct DevTables {
   void* ew = nullptr;      // T [6][4][3][9][n]     folded edge weights (scalar)
   void* eg = nullptr;      // T [6][4][3][9][2][n]  folded edge weights (vector)
   int* s0t = nullptr;      // [6][4][3][n]          first tap of every ghost point
+  int* ewin = nullptr;     // [24][nseg] int2       edge-kernel staging window per edge segment
+  int ewin_sp = 0, ewin_ts = 0, ewin_nseg = 0;
   void* egc = nullptr;     // T [6][4][3][9][2][2][n] curl halo weights (both components), on first use
   void* c2 = nullptr;      // T [6][nr][n][n] optional
   double* rad64 = nullptr; // FP64 copies for diagnostics
@@ -92,6 +94,7 @@ struct solar_ctx {
   int fp32 = 0;
   size_t esize = 8;
   int device = 0;
+  int nsm = 148;           // streaming multiprocessors of the device
   cudaStream_t stream = nullptr;
   void* A = nullptr;       // state
   void* B = nullptr;       // stage ping-pong
@@ -195,33 +198,35 @@ static bool make_map(const solar_ctx* c, const void* base, int bx, int by, CUten
   return r == CUDA_SUCCESS;
 }
 
-// Radial planes per edge-kernel CTA.  0 = choose from the grid size.
-#ifndef SOLAR_EDGE_PLANES
-#define SOLAR_EDGE_PLANES 0
-#endif
-
-template <typename T, int KC>
-static int launch_edge_kc(solar_ctx* c, const EdgeArgs<T>& a, int mode) {
-  const int nfl = mode == 1 ? c->g.nf : 3;
-  const size_t smem = (size_t)nfl * KC * 3 * c->g.n * sizeof(T);
-  if (smem > 48 * 1024) {
-    static bool attr_set = false;
-    if (!attr_set) {
-      CK(cudaFuncSetAttribute(edge_kernel<T, KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-      attr_set = true;
+// Staging windows of the edge kernel: the receiving edge is cut into segments of ts
+// positions (one thread per layer and position); a segment's ghost points read the source
+// positions [min s0t, max s0t + 9), widened to whole 16-byte pieces.
+static int edge_windows(solar_ctx* c) {
+  const int n = c->g.n, w16 = c->fp32 ? 4 : 2;
+  const int ts = std::min(n, 128), nseg = (n + ts - 1) / ts;
+  std::vector<int> win((size_t)24 * nseg * 2);
+  int sp = 0;
+  for (int fe = 0; fe < 24; ++fe)
+    for (int sg = 0; sg < nseg; ++sg) {
+      int lo = n, hi = 0;
+      for (int l = 0; l < 3; ++l)
+        for (int t = sg * ts; t < std::min(n, (sg + 1) * ts); ++t) {
+          const int s0 = c->ht.s0t[((size_t)fe * 3 + l) * n + t];
+          lo = std::min(lo, s0);
+          hi = std::max(hi, s0 + 9);
+        }
+      lo = lo / w16 * w16;
+      hi = std::min(n, (hi + w16 - 1) / w16 * w16);
+      win[((size_t)fe * nseg + sg) * 2 + 0] = lo;
+      win[((size_t)fe * nseg + sg) * 2 + 1] = hi - lo;
+      sp = std::max(sp, hi - lo);
     }
-  }
-  dim3 grid((c->g.nr + KC - 1) / KC, 4 * c->g.nface, c->g.nruns);
-  edge_kernel<T, KC><<<grid, 128, smem, c->stream>>>(a);
+  c->dt.ewin_sp = (sp + 7) / 8 * 8;       // 128-byte aligned tiles in shared memory
+  c->dt.ewin_ts = ts;
+  c->dt.ewin_nseg = nseg;
+  CK(cudaMalloc((void**)&c->dt.ewin, win.size() * sizeof(int)));
+  CK(cudaMemcpy(c->dt.ewin, win.data(), win.size() * sizeof(int), cudaMemcpyHostToDevice));
   return SOLAR_OK;
-}
-
-static int edge_planes(const solar_ctx* c) {
-  if (SOLAR_EDGE_PLANES > 0) return SOLAR_EDGE_PLANES;
-  const long long ctas4 = 4LL * c->g.nface * c->g.nruns * ((c->g.nr + 3) / 4);
-  if (ctas4 >= 148LL * 8) return 4;
-  if (2 * ctas4 >= 148LL * 8) return 2;
-  return 1;
 }
 
 template <typename T>
@@ -232,13 +237,33 @@ static int launch_edge(solar_ctx* c, void* buf, int mode, const int* active) {
   a.eg = (const T*)c->dt.eg;
   a.s0t = c->dt.s0t;
   a.active = active;
+  a.win = (const int2*)c->dt.ewin;
   a.g = c->g;
   a.mode = mode;
-  switch (edge_planes(c)) {
-    case 1: return launch_edge_kc<T, 1>(c, a, mode);
-    case 2: return launch_edge_kc<T, 2>(c, a, mode);
-    default: return launch_edge_kc<T, 4>(c, a, mode);
+  a.ts = c->dt.ewin_ts;
+  a.nseg = c->dt.ewin_nseg;
+  a.sp = c->dt.ewin_sp;
+  a.ngroups = mode == 1 ? (c->g.nf + 1) / 2 : 2;
+  // About one wave of resident CTAs, each marching at least 4 planes.
+  const long long per_chunk = 4LL * c->g.nface * a.ngroups * a.nseg * c->g.nruns;
+  const long long slots = (long long)c->nsm * EdgeMinBlocks<T>::value;
+  const long long nch = std::max<long long>(1, slots / per_chunk);
+  a.kchunk = std::max<int>(4, (int)((c->g.nr + nch - 1) / nch));
+  const size_t smem = (size_t)edge_smem_bytes(a.sp, a.ts, (int)sizeof(T));
+  // a tile box side is at most 256 values; each thread spreads at most one row
+  if (smem > 200 * 1024 || a.sp > 256 || 2 * a.sp > 3 * a.ts)
+    return fail(SOLAR_ERR_ARG, "edge staging window of %d positions is too wide", a.sp);
+  if (!make_map(c, buf, a.sp, 3, &a.mRow) || !make_map(c, buf, 4, a.sp, &a.mCol))
+    return fail(SOLAR_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+  a.err = c->err;
+  static bool attr_set = false;
+  if (!attr_set) {
+    CK(cudaFuncSetAttribute(edge_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    attr_set = true;
   }
+  dim3 grid((c->g.nr + a.kchunk - 1) / a.kchunk, 4 * c->g.nface * a.ngroups * a.nseg, c->g.nruns);
+  edge_kernel<T><<<grid, 3 * a.ts, smem, c->stream>>>(a);
+  return SOLAR_OK;
 }
 
 template <typename T, int TX, int TY, int MODE, bool HAS_RHO, bool FORCE = false>
@@ -390,7 +415,7 @@ static int check_device_error(solar_ctx* c) {
   CK(cudaStreamSynchronize(c->stream));
   if (h) {
     cudaMemsetAsync(c->err, 0, sizeof(int), c->stream);
-    if (h == 2) return fail(SOLAR_ERR_ARG, "forcing: a time sample outside the loaded samples was needed");
+    if (h == kErrForcingSample) return fail(SOLAR_ERR_ARG, "forcing: a time sample outside the loaded samples was needed");
     return fail(SOLAR_ERR_TIMEOUT, "a device wait gave up (code %d)", h);
   }
   return SOLAR_OK;
@@ -543,7 +568,7 @@ int solar_gpu_finalize(solar_ctx* c) {
   if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
   if (c->batch_graph) cudaGraphExecDestroy(c->batch_graph);
   void* ptrs[] = {c->A, c->B, c->W, c->stage64, c->part, c->red_out, c->active, c->target, c->done,
-                  c->err, c->dt.rad, c->dt.met, c->dt.ew, c->dt.eg, c->dt.egc, c->dt.s0t, c->dt.c2,
+                  c->err, c->dt.rad, c->dt.met, c->dt.ew, c->dt.eg, c->dt.egc, c->dt.s0t, c->dt.ewin, c->dt.c2,
                   c->dt.rad64, c->dt.vol2, c->dt.drw, c->dt.c2_64, c->dt.tanx, c->dt.gr};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -577,6 +602,7 @@ int solar_gpu_init(const solar_desc* d, solar_ctx** out) {
   c->device = d->device;
   cudaError_t ce = cudaSetDevice(c->device);
   if (ce != cudaSuccess) { delete c; return fail(SOLAR_ERR_CUDA, "cudaSetDevice(%d): %s", d->device, cudaGetErrorString(ce)); }
+  cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->device);
   c->fp32 = d->precision == SOLAR_FP32;
   c->esize = c->fp32 ? 4 : 8;
   Geom& g = c->g;
@@ -630,6 +656,7 @@ int solar_gpu_init(const solar_desc* d, solar_ctx** out) {
   else TRY(upload_tables<double>(c));
   TRYC(cudaMalloc((void**)&c->dt.s0t, c->ht.s0t.size() * sizeof(int)));
   TRYC(cudaMemcpy(c->dt.s0t, c->ht.s0t.data(), c->ht.s0t.size() * sizeof(int), cudaMemcpyHostToDevice));
+  TRY(edge_windows(c));
   TRYC(cudaMalloc((void**)&c->err, sizeof(int)));
   TRYC(cudaMemset(c->err, 0, sizeof(int)));
   if (!tensor_map_encoder()) { solar_gpu_finalize(c); return fail(SOLAR_ERR_CUDA, "cuTensorMapEncodeTiled entry point unavailable"); }

@@ -14,6 +14,16 @@ namespace solar {
 
 constexpr uint32_t kWaitLimit = 1u << 22;   // polls of try_wait before giving up
 
+// Codes a kernel leaves in the context's device error word.
+enum DeviceError : int {
+  kErrStageLead = 1,        // stage kernel: lead ring (p, v_r planes) wait gave up
+  kErrStageTile = 2,        // stage kernel: tile ring wait gave up
+  kErrFilterRing = 3,       // filter kernel: ring wait gave up
+  kErrEdgeRing = 4,         // edge kernel: ring wait gave up
+  kErrAdjointRing = 5,      // transposed stage kernel: ring wait gave up
+  kErrForcingSample = 16,   // a forcing time sample outside the loaded samples was needed
+};
+
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
@@ -60,17 +70,16 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
       : "memory");
 }
 
-// Asynchronous 4- or 8-byte global -> shared copy (no register staging); complete with
-// cp_async_wait_all() before the shared data is read.
-template <int BYTES>
-__device__ __forceinline__ void cp_async_small(void* dst, const void* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_u32(dst)), "l"(src), "n"(BYTES) : "memory");
-}
+// Asynchronous 16-byte global -> shared copy (no register staging, L2 only); complete
+// with cp_async_commit() and cp_async_wait<N>() before the shared data is read.
 __device__ __forceinline__ void cp_async_16(void* dst, const void* src) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
-__device__ __forceinline__ void cp_async_wait_all() {
-  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// wait until at most N of this thread's committed groups are still in flight
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
 __device__ __forceinline__ void tma_prefetch_desc(const CUtensorMap* map) {
