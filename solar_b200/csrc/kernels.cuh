@@ -42,15 +42,6 @@ struct Geom {
   __host__ __device__ long long at(int k, int j, int i) const {
     return (long long)k * plane + (long long)(JOFF + j) * pitch + IOFF + i;
   }
-  // Edge-line buffer ("strips"): for every face, edge, stored field and plane, the three
-  // source lines next to the edge that the neighbouring faces interpolate from --
-  //   S: rows j = 1..3, N: rows j = n-2..n-4, W: columns i = 1..3, E: columns i = n-2..n-4
-  // stored as strips[run][face][edge][slot][k][layer][t] with t along the edge.  It is the
-  // send buffer of the reference's halo exchange (temp(:,:,:,1:2) in derivative.f90).
-  __host__ __device__ long long strip(int run, int face, int edge, int s, int k, int l) const {
-    return (((((long long)(run * 6 + face) * 4 + edge) * nf + s) * nr + k) * 3 + l) * n;
-  }
-  __host__ __device__ long long strips_size() const { return (long long)nruns * 6 * 4 * nf * nr * 3 * n; }
 };
 
 struct EdgeRouteDev { int src_face, src_edge, reversed; };
@@ -837,27 +828,6 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) filter_kernel(const _
   }
   if (!ok && tid == 0)
     for (int q = 0; q < 1000; ++q) __nanosleep(1000);
-}
-
-// Fill the strip buffer of a whole buffer from its interior (after host uploads).
-template <typename T>
-__global__ void strip_extract_kernel(const T* __restrict__ q, T* __restrict__ strips, Geom g) {
-  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= g.strips_size()) return;
-  const int n = g.n;
-  const int t = idx % n;
-  long long r = idx / n;
-  const int l = r % 3; r /= 3;
-  const int k = r % g.nr; r /= g.nr;
-  const int s = r % g.nf; r /= g.nf;
-  const int e = r % 4; r /= 4;
-  const int face = r % 6, run = (int)(r / 6);
-  int ii, jj;
-  if (e == 0) { ii = t; jj = l + 1; }
-  else if (e == 1) { ii = t; jj = n - 2 - l; }
-  else if (e == 2) { ii = l + 1; jj = t; }
-  else { ii = n - 2 - l; jj = t; }
-  strips[idx] = q[g.vol(run, face, s) + g.at(k, jj, ii)];
 }
 
 // Edge lines exchanged between processes that own different zones: for item q the
