@@ -699,7 +699,9 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __
 // filter.f90:43), 11-point radial filter of the result; the 5 end planes at each radial
 // end become 0 (filter.f90:726-775).  A CTA owns a TX x TY column tile of one face and
 // one field and streams every plane through a kFilt-deep TMA ring, keeping the last 11
-// eta-filtered values of its column in registers.
+// eta-filtered values of its column in registers.  When the whole-column CTAs leave the
+// last wave of the GPU partly empty, the remaining columns are cut into radial chunks
+// (each re-reading the 5 planes on either side) that fill that wave.
 constexpr int kFiltRing = 4;
 
 template <typename T>
@@ -709,6 +711,8 @@ struct FilterArgs {
   const int* active;
   int* err;
   Geom g;
+  int whole;                // CTAs 0 .. whole-1 filter one (tile, field, face, run) unit each
+  int chunks;               // later CTAs filter one of `chunks` radial chunks of a unit
 };
 
 template <typename T, int TX, int TY>
@@ -735,10 +739,22 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) filter_kernel(const _
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L::BAR);
   const Geom& g = a.g;
   const int n = g.n, nr = g.nr;
-  const int tiles_x = n / TX;
-  const int i0 = (blockIdx.x % tiles_x) * TX, j0 = (blockIdx.x / tiles_x) * TY;
-  const int s = blockIdx.y;                  // stored field
-  const int run = blockIdx.z / g.nface, face = g.face0 + blockIdx.z % g.nface;
+  const int tiles_x = n / TX, tiles = tiles_x * (n / TY);
+  // unit = (tile, stored field, run and owned face); whole units first, then the radial
+  // chunks of the remaining units (output planes [ko0, ko1), input planes [ks, ke))
+  int unit = blockIdx.x, ko0 = 0, ko1 = nr;
+  if (unit >= a.whole) {
+    const int t = unit - a.whole, c = t % a.chunks;
+    unit = a.whole + t / a.chunks;
+    ko0 = c * nr / a.chunks;
+    ko1 = (c + 1) * nr / a.chunks;
+  }
+  const int ks = max(0, ko0 - 5), ke = min(nr, ko1 + 5);
+  const int tile = unit % tiles, rest = unit / tiles;
+  const int i0 = (tile % tiles_x) * TX, j0 = (tile / tiles_x) * TY;
+  const int s = rest % g.nf;                 // stored field
+  const int rz = rest / g.nf;
+  const int run = rz / g.nface, face = g.face0 + rz % g.nface;
   if (a.active && !a.active[run]) return;
   const int cx = threadIdx.x, ty = threadIdx.y, tid = ty * NT + cx;
   constexpr int PW = TX + 8;
@@ -755,7 +771,7 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) filter_kernel(const _
   }
   __syncthreads();
   if (tid == 0)
-    for (int k = 0; k < min(kFiltRing, nr); ++k) issue(k, k);
+    for (int k = ks; k < min(ks + kFiltRing, ke); ++k) issue(k, k - ks);
   T* out = a.qout + g.vol(run, face, s) + g.at(0, j0 + ty, i0 + V * cx);
   const T f0 = Coef<T>::filt(0), f1 = Coef<T>::filt(1), f2 = Coef<T>::filt(2), f3 = Coef<T>::filt(3);
   T tq[11][V];
@@ -769,11 +785,11 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) filter_kernel(const _
   bool ok = true;
   int slot = 0;
   uint32_t phase = 0;
-  for (int kb = 0; kb < nr && ok; kb += 11) {
+  for (int kb = ks; kb < ke && ok; kb += 11) {
 #pragma unroll
     for (int u = 0; u < 11; ++u) {
       const int k = kb + u;
-      if (k >= nr) break;
+      if (k >= ke) break;
       ok &= mbar_wait(&bars[slot], phase, a.err, kErrFilterRing);
       const T* bx = reinterpret_cast<const T*>(smem + slot * L::P_BYTES);
       T* t1 = reinterpret_cast<T*>(smem + kFiltRing * L::P_BYTES + (k & 1) * L::S_BYTES);
@@ -798,7 +814,7 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) filter_kernel(const _
         stv(t1 + r * TX + V * cx, v);
       }
       if (__syncthreads_or(!ok)) { ok = false; break; }
-      if (tid == 0 && k + kFiltRing < nr) issue(k + kFiltRing, slot);
+      if (tid == 0 && k + kFiltRing < ke) issue(k + kFiltRing, slot);
       if (++slot == kFiltRing) { slot = 0; phase ^= 1; }
       // eta filter of this thread's V points (rows ty .. ty+6 of the xi-filtered tile)
       T c[7][V];
@@ -807,7 +823,7 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) filter_kernel(const _
 #pragma unroll
       for (int q = 0; q < V; ++q)
         tq[u][q] = f0 * c[3][q] + f1 * (c[2][q] + c[4][q]) + f2 * (c[1][q] + c[5][q]) + f3 * (c[0][q] + c[6][q]);
-      if (k >= 10) {
+      if (k - ks >= 10) {
         // planes k-10 .. k sit at queue rows (u+1 .. u+11) % 11; the centre is k-5
         T v[V];
 #pragma unroll
@@ -824,7 +840,7 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) filter_kernel(const _
   // the five end planes at each radial end are zero (filter.f90:726-775)
   for (int m = 0; m < 10; ++m) {
     const int k = m < 5 ? m : nr - 10 + m;
-    stv(out + (long long)k * g.plane, zero);
+    if (k >= ko0 && k < ko1) stv(out + (long long)k * g.plane, zero);
   }
   if (!ok && tid == 0)
     for (int q = 0; q < 1000; ++q) __nanosleep(1000);

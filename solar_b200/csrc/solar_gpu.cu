@@ -356,12 +356,30 @@ static int launch_filter_t(solar_ctx* c, const void* qin, void* qout, const int*
   a.err = c->err;
   a.g = c->g;
   static bool attr_set = false;
+  static int resident = 1;
+  const int threads = (TX / Vec16<T>::V) * TY;
   if (!attr_set) {
     CK(cudaFuncSetAttribute(filter_kernel<T, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::TOTAL));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, filter_kernel<T, TX, TY>, threads, L::TOTAL));
+    resident = std::max(resident, 1);
     attr_set = true;
   }
-  dim3 grid((c->g.n / TX) * (c->g.n / TY), c->g.nf, c->g.nruns * c->g.nface);
-  filter_kernel<T, TX, TY><<<grid, dim3(TX / Vec16<T>::V, TY), L::TOTAL, c->stream>>>(a);
+  // Whole-column CTAs for every full wave; the units of a last, partial wave are cut into
+  // radial chunks (at least 11 planes each) so that they fill one wave.
+  const long long units = (long long)(c->g.n / TX) * (c->g.n / TY) * c->g.nf * c->g.nruns * c->g.nface;
+  const long long slots = (long long)c->nsm * resident;
+  const long long tail = units % slots;
+  a.whole = (int)units;
+  a.chunks = 1;
+  if (units > slots && tail > 0) {
+    const int chunks = (int)std::min<long long>(c->g.nr / 11, std::max<long long>(1, (slots + tail / 2) / tail));
+    if (chunks > 1) {
+      a.whole = (int)(units - tail);
+      a.chunks = chunks;
+    }
+  }
+  const long long grid = a.whole + (units - a.whole) * a.chunks;
+  filter_kernel<T, TX, TY><<<(unsigned)grid, dim3(TX / Vec16<T>::V, TY), L::TOTAL, c->stream>>>(a);
   return SOLAR_OK;
 }
 

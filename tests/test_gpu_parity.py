@@ -138,6 +138,21 @@ def test_filter_exp_random_fields_fp64(oracle_mod, c1_small):
         assert e < 1e-12, (name, e)
 
 
+def test_filter_exp_radial_chunks_fp64(oracle_mod):
+    """6 x 96^2 x 44 has 540 (tile, field, face) filter columns: more than the resident
+    filter CTAs of a 148-SM B200, so the columns of the last wave are filtered in radial
+    chunks that each re-read 5 planes on either side.  Random input makes every plane of a
+    chunk's halo count at full weight."""
+    cfg = configs.c1(nx=96, nr=44)
+    o = oracle_mod.Oracle(cfg)
+    q = random_state(o.state_shape, 6)
+    with Solver(cfg) as s:
+        qf = s.filter_exp(q)
+    for name, e in per_field(qf, o.filter_exp(q)).items():
+        assert e < 1e-12, (name, e)
+    assert np.all(qf[:, :, :5] == 0) and np.all(qf[:, :, -5:] == 0)
+
+
 # ---------------------------------------------------------------- time stepping
 def test_rk4_c1_100_steps_fp64(oracle_mod, c1_small):
     """Config 1 (6 x 32^3, 100 steps): per-field relative L2 <= 1e-11."""
