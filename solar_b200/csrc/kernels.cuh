@@ -158,7 +158,6 @@ __global__ void __launch_bounds__(384, (EdgeMinBlocks<T>::value)) edge_kernel(co
   const Geom& g = a.g;
   const int n = g.n, ts = a.ts, sp = a.sp;
   const int run = blockIdx.z;
-  if (a.active && !a.active[run]) return;
   const int kb = blockIdx.x * a.kchunk;
   if (kb >= g.nr) return;
   const int kc = min(a.kchunk, g.nr - kb);
@@ -282,6 +281,10 @@ __global__ void __launch_bounds__(384, (EdgeMinBlocks<T>::value)) edge_kernel(co
     mbar_fence_init();
   }
   __syncthreads();
+  // The previous kernel may still be finishing (programmatic launch): everything above
+  // reads constant tables only; the buffer and the run flags come after the wait.
+  grid_dependency_wait();
+  if (a.active && !a.active[run]) return;
   if (tid == 0)
     for (int d = 0; d < kEdgeDepth && d < kc; ++d) issue(d, d);
   mbar_wait(bars, 0, a.err, kErrEdgeRing);
@@ -432,7 +435,6 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __
   const int tiles_x = n / TX;
   const int i0 = (blockIdx.x % tiles_x) * TX, j0 = (blockIdx.x / tiles_x) * TY;
   const int run = blockIdx.z / g.nface, face = g.face0 + blockIdx.z % g.nface;
-  if (a.active && !a.active[run]) return;
   const int kb = blockIdx.y * a.kchunk;
   if (kb >= nr) return;
   const int ke = min(nr, kb + a.kchunk);
@@ -468,23 +470,7 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __
         tma_load_3d(t + L::X_BYTES + L::Y_BYTES + (QOFF + s) * L::O_BYTES, &a.mW, xO, yO, (zbase + s) * nr + k, b);
   };
 
-  if (tid == 0) {
-    for (int q = 0; q < kLead + kTile; ++q) mbar_init(&barL[q], 1);
-    mbar_fence_init();
-  }
-  __syncthreads();
-  // producer state (thread 0 only)
-  int m_issued = m_lo, slot_issue = 0;
-  if (tid == 0) {
-    tma_prefetch_desc(&a.mP);
-    for (; m_issued <= min(m_lo + kLead - 1, m_hi); ++m_issued) {
-      issue_lead(m_issued, slot_issue);
-      if (++slot_issue == kLead) slot_issue = 0;
-    }
-    for (int k = kb; k < min(kb + kTile, ke); ++k) issue_tile(k, k - kb);
-  }
-
-  // per-point constants
+  // per-point constants (constant tables: read before the dependency wait)
   const long long P2 = (long long)n * n;
   const int ib = i0 + V * cx, j = j0 + ty;
   const int p2 = j * n + ib;
@@ -498,6 +484,27 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __
   ldv(a.met + mTX * P2 + p2, m_TX);
   ldv(a.met + mTY * P2 + p2, m_TY);
   const T c1 = Coef<T>::drp(1), c2 = Coef<T>::drp(2), c3 = Coef<T>::drp(3);
+  if (tid == 0) {
+    for (int q = 0; q < kLead + kTile; ++q) mbar_init(&barL[q], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  // The previous kernel may still be finishing (programmatic launch): everything above
+  // reads constant tables only; the state, the run flags and the source term come after
+  // the wait.
+  grid_dependency_wait();
+  if (a.active && !a.active[run]) return;
+  // producer state (thread 0 only)
+  int m_issued = m_lo, slot_issue = 0;
+  if (tid == 0) {
+    tma_prefetch_desc(&a.mP);
+    for (; m_issued <= min(m_lo + kLead - 1, m_hi); ++m_issued) {
+      issue_lead(m_issued, slot_issue);
+      if (++slot_issue == kLead) slot_issue = 0;
+    }
+    for (int k = kb; k < min(kb + kTile, ke); ++k) issue_tile(k, k - kb);
+  }
+
   T f_xy[V];
   if (FORCE) ldv(a.force + (long long)face * P2 + p2, f_xy);
   const long long own = g.at(0, j, ib);
@@ -755,7 +762,6 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) filter_kernel(const _
   const int s = rest % g.nf;                 // stored field
   const int rz = rest / g.nf;
   const int run = rz / g.nface, face = g.face0 + rz % g.nface;
-  if (a.active && !a.active[run]) return;
   const int cx = threadIdx.x, ty = threadIdx.y, tid = ty * NT + cx;
   constexpr int PW = TX + 8;
   const int z0 = ((run * 6 + face) * g.nf + s) * nr;
@@ -770,6 +776,10 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) filter_kernel(const _
     mbar_fence_init();
   }
   __syncthreads();
+  // The previous kernel may still be finishing (programmatic launch): the input and the
+  // run flags are read only after the wait.
+  grid_dependency_wait();
+  if (a.active && !a.active[run]) return;
   if (tid == 0)
     for (int k = ks; k < min(ks + kFiltRing, ke); ++k) issue(k, k - ks);
   T* out = a.qout + g.vol(run, face, s) + g.at(0, j0 + ty, i0 + V * cx);

@@ -181,6 +181,26 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   return fn;
 }
 
+// Launch with programmatic stream serialization: the kernel starts as the previous kernel
+// in the stream retires its last CTAs, does its constant-table prologue, and waits on the
+// device (griddepcontrol.wait) before it touches anything that kernel wrote.  Used for the
+// stepping kernels, which all wait before reading the state, so the completion of each
+// implies that of the ones before.
+template <typename Args>
+static cudaError_t launch_pdl(void (*kernel)(Args), dim3 grid, dim3 block, size_t smem, cudaStream_t st, const Args& a) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, a);
+}
+
 // 3-D view of a whole buffer: x = padded column, y = padded row, z = plane index
 // ((run*6 + face)*nf + slot)*nr + k; box bx x by x 1.
 static bool make_map(const solar_ctx* c, const void* base, int bx, int by, CUtensorMap* m) {
@@ -262,7 +282,7 @@ static int launch_edge(solar_ctx* c, void* buf, int mode, const int* active) {
     attr_set = true;
   }
   dim3 grid((c->g.nr + a.kchunk - 1) / a.kchunk, 4 * c->g.nface * a.ngroups * a.nseg, c->g.nruns);
-  edge_kernel<T><<<grid, 3 * a.ts, smem, c->stream>>>(a);
+  CK(launch_pdl(edge_kernel<T>, grid, dim3(3 * a.ts), smem, c->stream, a));
   return SOLAR_OK;
 }
 
@@ -281,7 +301,7 @@ static int launch_stage_t(solar_ctx* c, StageArgs<T>& a, const void* qin) {
   }
   const int nchunks = (c->g.nr + a.kchunk - 1) / a.kchunk;
   dim3 grid((c->g.n / TX) * (c->g.n / TY), nchunks, c->g.nruns * c->g.nface);
-  stage_kernel<T, TX, TY, MODE, HAS_RHO, FORCE><<<grid, dim3(TX / Vec16<T>::V, TY), L::TOTAL, c->stream>>>(a);
+  CK(launch_pdl(stage_kernel<T, TX, TY, MODE, HAS_RHO, FORCE>, grid, dim3(TX / Vec16<T>::V, TY), L::TOTAL, c->stream, a));
   return SOLAR_OK;
 }
 
@@ -379,7 +399,7 @@ static int launch_filter_t(solar_ctx* c, const void* qin, void* qout, const int*
     }
   }
   const long long grid = a.whole + (units - a.whole) * a.chunks;
-  filter_kernel<T, TX, TY><<<(unsigned)grid, dim3(TX / Vec16<T>::V, TY), L::TOTAL, c->stream>>>(a);
+  CK(launch_pdl(filter_kernel<T, TX, TY>, dim3((unsigned)grid), dim3(TX / Vec16<T>::V, TY), L::TOTAL, c->stream, a));
   return SOLAR_OK;
 }
 
