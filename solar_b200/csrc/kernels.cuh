@@ -96,6 +96,32 @@ __device__ __forceinline__ void stv(T* p, const T* in) {
   *reinterpret_cast<VT*>(p) = v;
 }
 
+// Two floats in one 64-bit register for the paired FP32 arithmetic of sm_100
+// (add/mul/fma .f32x2: one instruction for both lanes, each rounded as the scalar one).
+__device__ __forceinline__ unsigned long long pk2(float x, float y) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(x), "f"(y));
+  return r;
+}
+__device__ __forceinline__ void upk2(unsigned long long r, float& x, float& y) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(x), "=f"(y) : "l"(r));
+}
+__device__ __forceinline__ unsigned long long add2(unsigned long long a, unsigned long long b) {
+  unsigned long long d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ unsigned long long mul2(unsigned long long a, unsigned long long b) {
+  unsigned long long d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigned long long b, unsigned long long c) {
+  unsigned long long d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+
 // ---------------------------------------------------------------------------------
 // Edge (ghost) kernel: INTERPOLATE_ALONG_X/Y + TRANSFORM_VECTOR_BETWEEN_MESHES_DIV + the
 // inter-zone exchange and its reversal, in one pass.  Every ghost value is a 9-tap sum
@@ -784,11 +810,17 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) filter_kernel(const _
     for (int k = ks; k < min(ks + kFiltRing, ke); ++k) issue(k, k - ks);
   T* out = a.qout + g.vol(run, face, s) + g.at(0, j0 + ty, i0 + V * cx);
   const T f0 = Coef<T>::filt(0), f1 = Coef<T>::filt(1), f2 = Coef<T>::filt(2), f3 = Coef<T>::filt(3);
+  // radial queue of eta-filtered planes; in float the four values of a thread are held as
+  // two packed pairs and the eta and radial filters run on pairs
+  constexpr bool PAIRS = sizeof(T) == 4;
   T tq[11][V];
+  unsigned long long tq2[11][2];
 #pragma unroll
-  for (int m = 0; m < 11; ++m)
+  for (int m = 0; m < 11; ++m) {
 #pragma unroll
     for (int q = 0; q < V; ++q) tq[m][q] = T(0);
+    tq2[m][0] = tq2[m][1] = 0ull;
+  }
   T zero[V];
 #pragma unroll
   for (int q = 0; q < V; ++q) zero[q] = T(0);
@@ -830,18 +862,47 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) filter_kernel(const _
       T c[7][V];
 #pragma unroll
       for (int m = 0; m < 7; ++m) ldv(t1 + (ty + m) * TX + V * cx, c[m]);
+      if constexpr (PAIRS) {
 #pragma unroll
-      for (int q = 0; q < V; ++q)
-        tq[u][q] = f0 * c[3][q] + f1 * (c[2][q] + c[4][q]) + f2 * (c[1][q] + c[5][q]) + f3 * (c[0][q] + c[6][q]);
+        for (int h = 0; h < 2; ++h) {
+          const float* cf = reinterpret_cast<const float*>(&c[0][0]);
+          auto pr = [&](int m) { return pk2(cf[m * V + 2 * h], cf[m * V + 2 * h + 1]); };
+          unsigned long long t = mul2(pk2(f0, f0), pr(3));
+          t = fma2(pk2(f1, f1), add2(pr(2), pr(4)), t);
+          t = fma2(pk2(f2, f2), add2(pr(1), pr(5)), t);
+          tq2[u][h] = fma2(pk2(f3, f3), add2(pr(0), pr(6)), t);
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < V; ++q)
+          tq[u][q] = f0 * c[3][q] + f1 * (c[2][q] + c[4][q]) + f2 * (c[1][q] + c[5][q]) + f3 * (c[0][q] + c[6][q]);
+      }
       if (k - ks >= 10) {
         // planes k-10 .. k sit at queue rows (u+1 .. u+11) % 11; the centre is k-5
         T v[V];
+        if constexpr (PAIRS) {
 #pragma unroll
-        for (int q = 0; q < V; ++q) {
-          T acc = Coef<T>::filtr(0) * tq[(u + 6) % 11][q];
+          for (int h = 0; h < 2; ++h) {
+            const float r0 = Coef<float>::filtr(0);
+            unsigned long long acc = mul2(pk2(r0, r0), tq2[(u + 6) % 11][h]);
 #pragma unroll
-          for (int m = 1; m <= 5; ++m) acc += Coef<T>::filtr(m) * (tq[(u + 6 - m) % 11][q] + tq[(u + 6 + m) % 11][q]);
-          v[q] = acc;
+            for (int m = 1; m <= 5; ++m) {
+              const float rm = Coef<float>::filtr(m);
+              acc = fma2(pk2(rm, rm), add2(tq2[(u + 6 - m) % 11][h], tq2[(u + 6 + m) % 11][h]), acc);
+            }
+            float x, y;
+            upk2(acc, x, y);
+            v[2 * h] = x;
+            v[2 * h + 1] = y;
+          }
+        } else {
+#pragma unroll
+          for (int q = 0; q < V; ++q) {
+            T acc = Coef<T>::filtr(0) * tq[(u + 6) % 11][q];
+#pragma unroll
+            for (int m = 1; m <= 5; ++m) acc += Coef<T>::filtr(m) * (tq[(u + 6 - m) % 11][q] + tq[(u + 6 + m) % 11][q]);
+            v[q] = acc;
+          }
         }
         stv(out + (long long)(k - 5) * g.plane, v);
       }
