@@ -153,6 +153,40 @@ def test_filter_exp_radial_chunks_fp64(oracle_mod):
     assert np.all(qf[:, :, :5] == 0) and np.all(qf[:, :, -5:] == 0)
 
 
+@pytest.fixture(scope="module")
+def c2_long_edges():
+    """6 x 144^2 x 24: the edge kernel cuts every 144-point edge into a 128-point segment and
+    a ragged 16-point one (whose idle threads must stay out of the staged window)."""
+    return configs.c2(nx=144, nr=24, nsteps=10)
+
+
+def test_long_edges_fp64(oracle_mod, c2_long_edges):
+    """COMPUTE_RHS (p and rotated-velocity halos) and FILTER_EXP (every field's halos) on
+    random input with segmented edges: relative L2 <= 1e-12 per field."""
+    o = oracle_mod.Oracle(c2_long_edges)
+    q = random_state(o.state_shape, 7)
+    with Solver(c2_long_edges) as s:
+        rhs = s.compute_rhs(q)
+        qf = s.filter_exp(q)
+    for name, e in per_field(rhs, o.compute_rhs(q)).items():
+        assert e < 1e-12, (name, e)
+    for name, e in per_field(qf, o.filter_exp(q)).items():
+        assert e < 1e-12, (name, e)
+
+
+def test_long_edges_rk4_fp32(oracle_mod, c2_long_edges):
+    """Ten FP32 steps (4 fields) with segmented edges against the FP64 oracle: <= 1e-5."""
+    o = oracle_mod.Oracle(c2_long_edges)
+    q0 = o.initial_state()
+    ref = o.rk4(q0, 10)
+    with Solver(c2_long_edges, precision="fp32", nfields=4) as s:
+        s.set_state(q0)
+        s.rk4(10)
+        q = s.get_state()
+    for name, e in per_field(q, ref, fields=(1, 2, 3, 4)).items():
+        assert e < 1e-5, (name, e)
+
+
 # ---------------------------------------------------------------- time stepping
 def test_rk4_c1_100_steps_fp64(oracle_mod, c1_small):
     """Config 1 (6 x 32^3, 100 steps): per-field relative L2 <= 1e-11."""
