@@ -369,13 +369,16 @@ __global__ void adj_rbdy_kernel(T* lout, const T* rb, const T* rad, Geom g, T dt
 // Transpose of the edge exchange, as a gather: every source-line point (the receiving face
 // and edge's route, layer l, position u along the source edge, plane k) sums the ghost
 // adjoints of the ghost points whose 9 taps include it -- a contiguous range of positions t,
-// tspan -- with the same folded coefficients, then adds the sum to its value (atomically:
-// the source lines of two edges of a face share their corner points).  mode 0: p scalar +
+// tspan -- then adds the sum to its value (atomically: the source lines of two edges of a
+// face share their corner points).  The weights come from a table transposed on the host,
+// wt[kind][row][j][u] = the folded coefficient with which ghost point t = lo(u) + j of
+// row (face-edge, layer) used source position u (kind 0 scalar, 1 and 2 the vector pair),
+// so the loop reads them contiguously across u with no tap-index lookup.  mode 0: p scalar +
 // the rotated vector component (v_xi on W/E receivers, v_eta on S/N); mode 1: every stored
 // field scalar.  grid: x over u, y over (receiving face-edge, layer), z over planes.
 template <typename T>
-__global__ void adj_edge_kernel(T* q, const T* __restrict__ ew, const T* __restrict__ eg, const int* __restrict__ s0t,
-                                const int* __restrict__ tspan, Geom g, int mode) {
+__global__ void adj_edge_kernel(T* q, const T* __restrict__ wt, int span, const int* __restrict__ tspan, Geom g,
+                                int mode) {
   const int n = g.n;
   const int u = blockIdx.x * blockDim.x + threadIdx.x;
   if (u >= n) return;
@@ -384,20 +387,22 @@ __global__ void adj_edge_kernel(T* q, const T* __restrict__ ew, const T* __restr
   const EdgeRouteDev rt = cRoute[face][e];
   const bool along_i = rt.src_edge <= 1;
   const int fixed = (rt.src_edge == 0 || rt.src_edge == 2) ? l + 1 : n - 2 - l;
-  const int row = fe * 3 + l, crow = row * 9;
+  const int row = fe * 3 + l;
   const int lo = __ldg(tspan + (row * n + u) * 2), hi = __ldg(tspan + (row * n + u) * 2 + 1);
   if (hi < lo) return;
   const long long src = g.at(k, along_i ? fixed : u, along_i ? u : fixed);
   // receiver ghost position of (e, l, t): rows -1-l / n+l, columns -1-l / n+l
-  const long long g0 = (e == 0) ? g.at(k, -1 - l, 0) : (e == 1) ? g.at(k, n + l, 0)
-                     : (e == 2) ? g.at(k, 0, -1 - l) : g.at(k, 0, n + l);
+  const long long g0 = ((e == 0) ? g.at(k, -1 - l, 0) : (e == 1) ? g.at(k, n + l, 0)
+                      : (e == 2) ? g.at(k, 0, -1 - l) : g.at(k, 0, n + l)) + (long long)lo * (e <= 1 ? 1 : g.pitch);
   const long long gstep = e <= 1 ? 1 : g.pitch;
-  const int* st = s0t + row * n;
+  const long long kind = 72LL * span * n;                 // stride between weight kinds
+  const T* w = wt + (long long)row * span * n + u;        // weight of ghost lo + j at w[j * n]
+  const int cnt = hi - lo + 1;
   if (mode == 1) {
     for (int sl = 0; sl < g.nf; ++sl) {
       const T* gv = q + g.vol(0, face, sl) + g0;
       T acc = T(0);
-      for (int t = lo; t <= hi; ++t) acc += __ldg(ew + (long long)(crow + u - __ldg(st + t)) * n + t) * gv[t * gstep];
+      for (int j = 0; j < cnt; ++j) acc += __ldg(w + j * n) * gv[j * gstep];
       atomicAdd(q + g.vol(0, rt.src_face, sl) + src, acc);
     }
     return;
@@ -405,12 +410,11 @@ __global__ void adj_edge_kernel(T* q, const T* __restrict__ ew, const T* __restr
   const T* gp = q + g.vol(0, face, g.slot[kP]) + g0;
   const T* gvv = q + g.vol(0, face, e >= 2 ? g.slot[kVxi] : g.slot[kVeta]) + g0;
   T ap = T(0), ax = T(0), ay = T(0);
-  for (int t = lo; t <= hi; ++t) {
-    const int r = crow + u - __ldg(st + t);
-    const T pv = gp[t * gstep], vv = gvv[t * gstep];
-    ap += __ldg(ew + (long long)r * n + t) * pv;
-    ax += __ldg(eg + ((long long)r * 2 + 0) * n + t) * vv;
-    ay += __ldg(eg + ((long long)r * 2 + 1) * n + t) * vv;
+  for (int j = 0; j < cnt; ++j) {
+    const T pv = gp[j * gstep], vv = gvv[j * gstep];
+    ap += __ldg(w + j * n) * pv;
+    ax += __ldg(w + kind + j * n) * vv;
+    ay += __ldg(w + 2 * kind + j * n) * vv;
   }
   atomicAdd(q + g.vol(0, rt.src_face, g.slot[kP]) + src, ap);
   atomicAdd(q + g.vol(0, rt.src_face, g.slot[kVxi]) + src, ax);

@@ -25,6 +25,28 @@ static int adj_alloc(solar_ctx* c) {
   CK(cudaMalloc(&b.rb, (size_t)6 * 4 * 2 * c->g.n * c->g.n * c->esize));
   CK(cudaMalloc((void**)&b.tspan, c->ht.tspan.size() * sizeof(int)));
   CK(cudaMemcpy(b.tspan, c->ht.tspan.data(), c->ht.tspan.size() * sizeof(int), cudaMemcpyHostToDevice));
+  // Edge weights transposed to the gather's order: wt[kind][row][j][u] is the coefficient
+  // with which ghost point t = lo(u) + j of row (face-edge, layer) used source position u
+  // (kind 0: scalar weight, 1 and 2: the vector pair); zero past the ghost range of u.
+  const int n = c->g.n;
+  int span = 1;
+  for (size_t q = 0; q < c->ht.tspan.size(); q += 2) span = std::max(span, c->ht.tspan[q + 1] - c->ht.tspan[q] + 1);
+  std::vector<double> wt((size_t)3 * 72 * span * n, 0.0);
+  for (int row = 0; row < 72; ++row)
+    for (int u = 0; u < n; ++u) {
+      const int lo = c->ht.tspan[((size_t)row * n + u) * 2], hi = c->ht.tspan[((size_t)row * n + u) * 2 + 1];
+      for (int t = lo; t <= hi; ++t) {
+        const int s = u - c->ht.s0t[(size_t)row * n + t];
+        if (s < 0 || s > 8) continue;
+        const size_t tap = (size_t)row * 9 + s, o = ((size_t)row * span + (t - lo)) * n + u;
+        wt[o] = c->ht.ew[tap * n + t];
+        wt[(size_t)72 * span * n + o] = c->ht.eg[(tap * 2 + 0) * n + t];
+        wt[(size_t)2 * 72 * span * n + o] = c->ht.eg[(tap * 2 + 1) * n + t];
+      }
+    }
+  int rc = c->fp32 ? upload<float>(&b.wt, wt) : upload<double>(&b.wt, wt);
+  if (rc) return rc;
+  b.wt_span = span;
   return SOLAR_OK;
 }
 
@@ -107,7 +129,7 @@ static int enqueue_rhs_adjoint(solar_ctx* c, AdjStageArgs<T> a) {
   adj_rbdy_kernel<T><<<blocks_for(6LL * 14 * g.n * g.n, 256), 256, 0, c->stream>>>((T*)b.T1, (const T*)b.rb,
                                                                                    (const T*)c->dt.rad, g, a.dt);
   adj_edge_kernel<T><<<dim3(blocks_for(g.n, 128), 72, g.nr), 128, 0, c->stream>>>(
-      (T*)b.T1, (const T*)c->dt.ew, (const T*)c->dt.eg, c->dt.s0t, b.tspan, g, 0);
+      (T*)b.T1, (const T*)b.wt, b.wt_span, b.tspan, g, 0);
   CK(cudaGetLastError());
   std::swap(b.L, b.T1);
   std::swap(b.LW, b.T2);
@@ -128,7 +150,7 @@ static int enqueue_filter_adjoint(solar_ctx* c) {
   else
     adj_filter_xy_kernel<T, 16, 16, KP><<<dim3((g.n / 16) * (g.n / 16), kch, 6 * g.nf), 256, 0, c->stream>>>(T1, L, g);
   adj_edge_kernel<T><<<dim3(blocks_for(g.n, 128), 72, g.nr), 128, 0, c->stream>>>(
-      L, (const T*)c->dt.ew, (const T*)c->dt.eg, c->dt.s0t, c->adj.tspan, g, 1);
+      L, (const T*)c->adj.wt, c->adj.wt_span, c->adj.tspan, g, 1);
   CK(cudaGetLastError());
   return SOLAR_OK;
 }

@@ -67,6 +67,8 @@ struct AdjBuffers {
   void* T2 = nullptr;
   void* rb = nullptr;       // R1, R2 of the one-sided radial rows (planes 1, 2, nr-3, nr-2)
   int* tspan = nullptr;     // ghost-point range of every source position (transposed exchange)
+  void* wt = nullptr;       // T [3][72][wt_span][n] edge weights in the gather's order
+  int wt_span = 0;
   double* grad = nullptr;   // dJ/dc, compact [face][k][j][i]
   void* ckpt = nullptr;     // state checkpoints (padded copies of the state buffer)
   size_t ckpt_bytes = 0;
@@ -610,7 +612,7 @@ int solar_gpu_finalize(solar_ctx* c) {
                   c->dt.rad64, c->dt.vol2, c->dt.drw, c->dt.c2_64, c->dt.tanx, c->dt.gr};
   for (void* p : ptrs)
     if (p) cudaFree(p);
-  void* aptrs[] = {c->adj.L, c->adj.LW, c->adj.T1, c->adj.T2, c->adj.rb, c->adj.tspan, c->adj.grad, c->adj.ckpt, c->adj.ckpt2,
+  void* aptrs[] = {c->adj.L, c->adj.LW, c->adj.T1, c->adj.T2, c->adj.rb, c->adj.tspan, c->adj.wt, c->adj.grad, c->adj.ckpt, c->adj.ckpt2,
                    c->adj.div, c->adj.traces, c->adj.rec_off, c->adj.rec_w, c->adj.clk, c->split_items, c->split_slots,
                    c->force_clock, c->force_exy, c->force_samples, c->force_xy, c->force_r};
   for (void* p : aptrs)
