@@ -1015,7 +1015,53 @@ __global__ void gaussian_kernel(double* p, Geom g, int face, const double* tanx,
 }
 
 // ---------------------------------------------------------------------------------
-// FP64 reductions for norm / diagnostics.  Stage 1: one CTA per (face, k) plane writes
+// Sum of squares of one stored field, for the per-step norm (auxiliary.f90:100-125): one
+// CTA per (owned face, plane) adds its plane in FP64 (a warp per row, 16-byte loads) and
+// writes one partial; sumsq_final_kernel adds the partials in a fixed order.
+template <typename T>
+__global__ void sumsq_plane_kernel(const T* __restrict__ q, Geom g, int run, int slot, double* part) {
+  constexpr int V = Vec16<T>::V;
+  const int face = g.face0 + blockIdx.x / g.nr, k = blockIdx.x % g.nr;
+  const int n = g.n, per_row = n / V;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const T* base = q + g.vol(run, face, slot) + g.at(k, 0, 0);
+  double acc = 0.0;
+  for (int j = warp; j < n; j += nwarp) {
+    const T* row = base + (long long)j * g.pitch;
+    for (int c = lane; c < per_row; c += 32) {
+      T v[V];
+      ldv(row + c * V, v);
+#pragma unroll
+      for (int m = 0; m < V; ++m) acc = fma((double)v[m], (double)v[m], acc);
+    }
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  __shared__ double red[32];
+  if (lane == 0) red[warp] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < nwarp; ++w) t += red[w];
+    part[blockIdx.x] = t;
+  }
+}
+
+__global__ void sumsq_final_kernel(const double* __restrict__ part, int nblocks, double* out) {
+  __shared__ double red[256];
+  double acc = 0.0;
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) acc += part[b];
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if ((int)threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[0] = red[0];
+}
+
+// ---------------------------------------------------------------------------------
+// FP64 reductions for the diagnostics.  Stage 1: one CTA per (face, k) plane writes
 // 5 partials; stage 2: one CTA sums them in a fixed order (deterministic).
 //   part[0] = sum f_sel^2, [1] = energy, [2] = mass, [3] = max |p|, [4] = non-finite count
 template <typename T>

@@ -566,6 +566,22 @@ static int reduce(solar_ctx* c, int run, int sel_field, double* out5) {
   return SOLAR_OK;
 }
 
+// Sum of squares of reference field sel_field (0-based) of one run over the owned zones;
+// zero for a field the context does not store.
+static int sumsq(solar_ctx* c, int run, int sel_field, double* out) {
+  const int s = c->g.slot[sel_field];
+  if (s < 0) { *out = 0.0; return SOLAR_OK; }
+  const int nblocks = c->g.nface * c->g.nr;
+  if (c->fp32) sumsq_plane_kernel<float><<<nblocks, 256, 0, c->stream>>>((const float*)c->A, c->g, run, s, c->part);
+  else sumsq_plane_kernel<double><<<nblocks, 256, 0, c->stream>>>((const double*)c->A, c->g, run, s, c->part);
+  CK(cudaGetLastError());
+  sumsq_final_kernel<<<1, 256, 0, c->stream>>>(c->part, nblocks, c->red_out);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, c->red_out, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return SOLAR_OK;
+}
+
 }  // namespace solar
 
 // ===================================================================== C-ABI
@@ -900,10 +916,10 @@ int solar_gpu_norm(solar_ctx* c, int run, int field, double* out) {
   int rc = check_ctx(c);
   if (rc) return rc;
   if (!out || field < 1 || field > 5 || run < 0 || run >= c->g.nruns) return fail(SOLAR_ERR_ARG, "bad field/run");
-  double r[5];
-  if ((rc = reduce(c, run, field - 1, r))) return rc;
+  double ss = 0.0;
+  if ((rc = sumsq(c, run, field - 1, &ss))) return rc;
   // auxiliary.f90:122
-  *out = std::pow(r[0] / ((double)c->g.n * c->g.n * c->g.nr) * 6.0, 0.5);
+  *out = std::pow(ss / ((double)c->g.n * c->g.n * c->g.nr) * 6.0, 0.5);
   return SOLAR_OK;
 }
 
