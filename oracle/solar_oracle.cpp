@@ -494,16 +494,14 @@ void convert_xe_tp(const oracle_ctx& c, int z, const double* axi, const double* 
 void transform_div(const oracle_ctx& c, int z, const double* th, const double* ph, double* out) {
   const int n = c.nx;
   const size_t ss = (size_t)c.nr * 3 * n;
-  double X[7], Y[7], C[7], D[7];  // index m+3, m = -3..3
+  double X[7], Y[7], C[7];  // index m+3, m = -3..3
   for (int i = 1; i <= NST; ++i) {
     X[3 - i] = std::tan(c.gxi[0] - i * c.dxi);
     Y[3 - i] = std::tan(c.geta[0] - i * c.deta);
     C[3 - i] = std::sqrt(1.0 + X[3 - i] * X[3 - i]);
-    D[3 - i] = std::sqrt(1.0 + Y[3 - i] * Y[3 - i]);
     X[3 + i] = std::tan(c.gxi[n - 1] + i * c.dxi);
     Y[3 + i] = std::tan(c.geta[n - 1] + i * c.deta);
     C[3 + i] = std::sqrt(1.0 + X[3 + i] * X[3 + i]);
-    D[3 + i] = std::sqrt(1.0 + Y[3 + i] * Y[3 + i]);
   }
   std::vector<double> gD(n);
   for (int i = 0; i < n; ++i) gD[i] = std::pow(1.0 + std::pow(std::tan(c.geta[i]), 2.0), 0.5);

@@ -70,18 +70,6 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
       : "memory");
 }
 
-// Asynchronous 16-byte global -> shared copy (no register staging, L2 only); complete
-// with cp_async_commit() and cp_async_wait<N>() before the shared data is read.
-__device__ __forceinline__ void cp_async_16(void* dst, const void* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-// wait until at most N of this thread's committed groups are still in flight
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
 // Programmatic dependent launch.  A kernel launched with programmatic stream serialization
 // starts as its predecessor's last CTAs exit, before that grid has fully completed; it must
 // call grid_dependency_wait() before it reads anything the predecessor (or an earlier
