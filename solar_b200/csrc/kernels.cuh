@@ -96,6 +96,17 @@ __device__ __forceinline__ void stv(T* p, const T* in) {
   *reinterpret_cast<VT*>(p) = v;
 }
 
+// One 32-byte sector in a single 256-bit store (sm_100); p must be 32-byte aligned.
+__device__ __forceinline__ void st_sector(float* p, const float* v) {
+  asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "f"(v[0]), "f"(v[1]), "f"(v[2]),
+               "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7])
+               : "memory");
+}
+__device__ __forceinline__ void st_sector(double* p, const double* v) {
+  asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(v[0]), "d"(v[1]), "d"(v[2]), "d"(v[3])
+               : "memory");
+}
+
 // Two floats in one 64-bit register for the paired FP32 arithmetic of sm_100
 // (add/mul/fma .f32x2: one instruction for both lanes, each rounded as the scalar one).
 __device__ __forceinline__ unsigned long long pk2(float x, float y) {
@@ -290,8 +301,7 @@ __global__ void __launch_bounds__(384, (EdgeMinBlocks<T>::value)) edge_kernel(co
 #pragma unroll
       for (int ll = 0; ll < 3; ++ll) sect[ll] = r[ll * ts];
     }
-    stv(d, sect);
-    stv(d + Vec16<T>::V, sect + Vec16<T>::V);
+    st_sector(d, sect);
   };
   auto sectors = [&](int half) {                         // W/E: one whole sector per row
     if (writer) {
