@@ -370,48 +370,72 @@ __global__ void adj_rbdy_kernel(T* lout, const T* rb, const T* rad, Geom g, T dt
 // and edge's route, layer l, position u along the source edge, plane k) sums the ghost
 // adjoints of the ghost points whose 9 taps include it -- a contiguous range of positions t,
 // tspan -- then adds the sum to its value (atomically: the source lines of two edges of a
-// face share their corner points).  The weights come from a table transposed on the host,
-// wt[kind][row][j][u] = the folded coefficient with which ghost point t = lo(u) + j of
-// row (face-edge, layer) used source position u (kind 0 scalar, 1 and 2 the vector pair),
-// so the loop reads them contiguously across u with no tap-index lookup.  mode 0: p scalar +
-// the rotated vector component (v_xi on W/E receivers, v_eta on S/N); mode 1: every stored
-// field scalar.  grid: x over u, y over (receiving face-edge, layer), z over planes.
+// face share their corner points).  The CTA first copies the ghost values its positions
+// need (the union of their ranges, one read per ghost point and field) into shared memory:
+// on W/E receivers those are column entries, one scattered request each.  The weights come
+// from a table transposed on the host, wt[kind][row][j][u] = the folded coefficient with
+// which ghost point t = lo(u) + j of row (face-edge, layer) used source position u (kind 0
+// scalar, 1 and 2 the vector pair), read contiguously across u.  mode 0: p scalar + the
+// rotated vector component (v_xi on W/E receivers, v_eta on S/N); mode 1: every stored
+// field scalar.  grid: x over u, y over (receiving face-edge, layer), z over planes; dynamic
+// shared memory: (mode 0 ? 2 : nf) x n values.
 template <typename T>
 __global__ void adj_edge_kernel(T* q, const T* __restrict__ wt, int span, const int* __restrict__ tspan, Geom g,
                                 int mode) {
+  extern __shared__ __align__(16) unsigned char aesm[];
+  T* const sg = reinterpret_cast<T*>(aesm);               // [field][t]
+  __shared__ int s_lo, s_hi;
   const int n = g.n;
   const int u = blockIdx.x * blockDim.x + threadIdx.x;
-  if (u >= n) return;
   const int fe = blockIdx.y / 3, l = blockIdx.y % 3, k = blockIdx.z;
   const int face = fe >> 2, e = fe & 3;
   const EdgeRouteDev rt = cRoute[face][e];
   const bool along_i = rt.src_edge <= 1;
   const int fixed = (rt.src_edge == 0 || rt.src_edge == 2) ? l + 1 : n - 2 - l;
   const int row = fe * 3 + l;
-  const int lo = __ldg(tspan + (row * n + u) * 2), hi = __ldg(tspan + (row * n + u) * 2 + 1);
+  int lo = 0, hi = -1;
+  if (u < n) {
+    lo = __ldg(tspan + (row * n + u) * 2);
+    hi = __ldg(tspan + (row * n + u) * 2 + 1);
+  }
+  if (threadIdx.x == 0) { s_lo = n; s_hi = -1; }
+  __syncthreads();
+  if (hi >= lo) { atomicMin(&s_lo, lo); atomicMax(&s_hi, hi); }
+  __syncthreads();
+  const int tmin = s_lo, tmax = s_hi;
+  if (tmax < tmin) return;                                 // no ghost point uses this block
+  // receiver ghost position of (e, l, t): rows -1-l / n+l, columns -1-l / n+l
+  const long long g0 = (e == 0) ? g.at(k, -1 - l, 0) : (e == 1) ? g.at(k, n + l, 0)
+                     : (e == 2) ? g.at(k, 0, -1 - l) : g.at(k, 0, n + l);
+  const long long gstep = e <= 1 ? 1 : g.pitch;
+  const int nfs = mode == 1 ? g.nf : 2;
+  auto slot_of = [&](int f) {
+    return mode == 1 ? f : (f == 0 ? g.slot[kP] : (e >= 2 ? g.slot[kVxi] : g.slot[kVeta]));
+  };
+  for (int f = 0; f < nfs; ++f) {
+    const T* gv = q + g.vol(0, face, slot_of(f)) + g0;
+    for (int t = tmin + threadIdx.x; t <= tmax; t += blockDim.x) sg[f * n + t] = gv[t * gstep];
+  }
+  __syncthreads();
   if (hi < lo) return;
   const long long src = g.at(k, along_i ? fixed : u, along_i ? u : fixed);
-  // receiver ghost position of (e, l, t): rows -1-l / n+l, columns -1-l / n+l
-  const long long g0 = ((e == 0) ? g.at(k, -1 - l, 0) : (e == 1) ? g.at(k, n + l, 0)
-                      : (e == 2) ? g.at(k, 0, -1 - l) : g.at(k, 0, n + l)) + (long long)lo * (e <= 1 ? 1 : g.pitch);
-  const long long gstep = e <= 1 ? 1 : g.pitch;
   const long long kind = 72LL * span * n;                 // stride between weight kinds
   const T* w = wt + (long long)row * span * n + u;        // weight of ghost lo + j at w[j * n]
   const int cnt = hi - lo + 1;
   if (mode == 1) {
-    for (int sl = 0; sl < g.nf; ++sl) {
-      const T* gv = q + g.vol(0, face, sl) + g0;
+    for (int f = 0; f < nfs; ++f) {
+      const T* gs = sg + f * n + lo;
       T acc = T(0);
-      for (int j = 0; j < cnt; ++j) acc += __ldg(w + j * n) * gv[j * gstep];
-      atomicAdd(q + g.vol(0, rt.src_face, sl) + src, acc);
+      for (int j = 0; j < cnt; ++j) acc += __ldg(w + j * n) * gs[j];
+      atomicAdd(q + g.vol(0, rt.src_face, f) + src, acc);
     }
     return;
   }
-  const T* gp = q + g.vol(0, face, g.slot[kP]) + g0;
-  const T* gvv = q + g.vol(0, face, e >= 2 ? g.slot[kVxi] : g.slot[kVeta]) + g0;
+  const T* gp = sg + lo;
+  const T* gvv = sg + n + lo;
   T ap = T(0), ax = T(0), ay = T(0);
   for (int j = 0; j < cnt; ++j) {
-    const T pv = gp[j * gstep], vv = gvv[j * gstep];
+    const T pv = gp[j], vv = gvv[j];
     ap += __ldg(w + j * n) * pv;
     ax += __ldg(w + kind + j * n) * vv;
     ay += __ldg(w + 2 * kind + j * n) * vv;

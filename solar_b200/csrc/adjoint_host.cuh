@@ -128,7 +128,7 @@ static int enqueue_rhs_adjoint(solar_ctx* c, AdjStageArgs<T> a) {
   if (rc) return rc;
   adj_rbdy_kernel<T><<<blocks_for(6LL * 14 * g.n * g.n, 256), 256, 0, c->stream>>>((T*)b.T1, (const T*)b.rb,
                                                                                    (const T*)c->dt.rad, g, a.dt);
-  adj_edge_kernel<T><<<dim3(blocks_for(g.n, 128), 72, g.nr), 128, 0, c->stream>>>(
+  adj_edge_kernel<T><<<dim3(blocks_for(g.n, 128), 72, g.nr), 128, 2 * g.n * sizeof(T), c->stream>>>(
       (T*)b.T1, (const T*)b.wt, b.wt_span, b.tspan, g, 0);
   CK(cudaGetLastError());
   std::swap(b.L, b.T1);
@@ -149,7 +149,7 @@ static int enqueue_filter_adjoint(solar_ctx* c) {
     adj_filter_xy_kernel<T, 32, 8, KP><<<dim3((g.n / 32) * (g.n / 8), kch, 6 * g.nf), 256, 0, c->stream>>>(T1, L, g);
   else
     adj_filter_xy_kernel<T, 16, 16, KP><<<dim3((g.n / 16) * (g.n / 16), kch, 6 * g.nf), 256, 0, c->stream>>>(T1, L, g);
-  adj_edge_kernel<T><<<dim3(blocks_for(g.n, 128), 72, g.nr), 128, 0, c->stream>>>(
+  adj_edge_kernel<T><<<dim3(blocks_for(g.n, 128), 72, g.nr), 128, g.nf * g.n * sizeof(T), c->stream>>>(
       L, (const T*)c->adj.wt, c->adj.wt_span, c->adj.tspan, g, 1);
   CK(cudaGetLastError());
   return SOLAR_OK;
