@@ -330,10 +330,12 @@ static int launch_stage_mode(solar_ctx* c, StageArgs<T>& a, const void* qin, int
   }
 }
 
-// Stage tiles (TX x TY points).  The default is 32 x 16 in float and 32 x 8 in double;
-// 16 x 16 when nx is not a multiple of 32.
+// Stage tiles (TX x TY points).  The default is 64 x 8 when nx is a multiple of 64 (the
+// fastest shape measured at 64^3, 128^3 and 384^3 in both precisions), else 32 x 16 in
+// float and 32 x 8 in double, and 16 x 16 when nx is not a multiple of 32.
 static void default_tile(int n, bool fp32, int* tx, int* ty) {
   if (n % 32) { *tx = 16; *ty = 16; return; }
+  if (n % 64 == 0) { *tx = 64; *ty = 8; return; }
   *tx = 32;
   *ty = fp32 ? 16 : 8;
 }
@@ -685,10 +687,19 @@ int solar_gpu_init(const solar_desc* d, solar_ctx** out) {
   }
   if (d->kchunk > 0) c->kchunk = d->kchunk;
   else {
+    // Radial planes per stage CTA.  Measured best on B200: about nr/3 in float and nr/6 in
+    // double, between 16 and 64 (43 / 22 at 128^3, 64 at 384^3, ~21 at 64 runs of 64^3).
+    // Grids too small to fill one wave of two CTAs per SM that way get about four waves.
     const long long blocks = 6LL * g.nruns * (g.n / c->tile_x) * (g.n / c->tile_y);
-    const long long want = 148LL * 2 * 4;   // about four waves of two resident CTAs per SM
-    int nch = (int)std::max<long long>(1, (want + blocks - 1) / blocks);
-    c->kchunk = std::max(8, (g.nr + nch - 1) / nch);
+    int kc = std::min(64, std::max(16, c->fp32 ? g.nr / 3 : g.nr / 6));
+    int nch = (g.nr + kc - 1) / kc;
+    if (blocks * nch < 148LL * 2) {
+      const long long want = 148LL * 2 * 4;
+      nch = (int)std::max<long long>(1, (want + blocks - 1) / blocks);
+      c->kchunk = std::max(8, (g.nr + nch - 1) / nch);
+    } else {
+      c->kchunk = (g.nr + nch - 1) / nch;
+    }
   }
 #define TRY(x) do { int rc_ = (x); if (rc_) { solar_gpu_finalize(c); return rc_; } } while (0)
 #define TRYC(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) { std::string m_ = cudaGetErrorString(e_); solar_gpu_finalize(c); return fail(e_ == cudaErrorMemoryAllocation ? SOLAR_ERR_NOMEM : SOLAR_ERR_CUDA, "%s: %s", #call, m_.c_str()); } } while (0)
