@@ -101,8 +101,10 @@ int solar_gpu_add_gaussian(solar_ctx* c, int run, double x0, double y0, double z
  * stages of COMPUTE_RHS + BC_RHS + SPONGE + update, then FILTER_EXP -- on every run. */
 int solar_gpu_rk4(solar_ctx* c, int nsteps);
 
-/* Batched RK4: run r advances nsteps_per_run[r] steps (uneven counts), all runs in the
- * same launches, replayed from one captured CUDA graph. */
+/* Batched RK4: run r advances nsteps_per_run[r] steps (uneven counts), all live runs in the
+ * same launches.  Runs are ordered by step count; each stretch of steps with the same number
+ * of live runs replays one captured CUDA graph whose grids cover only those runs (graphs are
+ * kept per live-run count). */
 int solar_gpu_rk4_runs(solar_ctx* c, const int* nsteps_per_run);
 
 /* solar_gpu_rk4_runs, plus the device time of the whole batch (CUDA events on the

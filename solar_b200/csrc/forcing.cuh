@@ -197,7 +197,7 @@ int solar_gpu_set_forcing(solar_ctx* c, int kind, int k_center, int nstep) {
   }
   c->forcing = kind;
   if (c->step_graph) { cudaGraphExecDestroy(c->step_graph); c->step_graph = nullptr; }
-  if (c->batch_graph) { cudaGraphExecDestroy(c->batch_graph); c->batch_graph = nullptr; }
+  drop_batch_graphs(c);
   return SOLAR_OK;
 }
 

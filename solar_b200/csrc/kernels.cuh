@@ -149,7 +149,7 @@ struct EdgeArgs {
   const T* ew;              // [6][4][3][9][n]     scalar tap weights, position fastest
   const T* eg;              // [6][4][3][9][2][n]  vector tap weights (v_xi, v_eta)
   const int* s0t;           // [6][4][3][n]        first tap along the source edge
-  const int* active;        // per-run flag or nullptr
+  const int* runs;          // stored run of each launched run index (grid z), or nullptr
   const int2* win;          // [24][nseg] staged source window (first position, count)
   Geom g;
   int mode;
@@ -194,7 +194,8 @@ __global__ void __launch_bounds__(384, (EdgeMinBlocks<T>::value)) edge_kernel(co
   extern __shared__ __align__(128) unsigned char esm[];
   const Geom& g = a.g;
   const int n = g.n, ts = a.ts, sp = a.sp;
-  const int run = blockIdx.z;
+  // the run map is written before the launches that use it and constant during them
+  const int run = a.runs ? a.runs[blockIdx.z] : blockIdx.z;
   const int kb = blockIdx.x * a.kchunk;
   if (kb >= g.nr) return;
   const int kc = min(a.kchunk, g.nr - kb);
@@ -318,9 +319,8 @@ __global__ void __launch_bounds__(384, (EdgeMinBlocks<T>::value)) edge_kernel(co
   }
   __syncthreads();
   // The previous kernel may still be finishing (programmatic launch): everything above
-  // reads constant tables only; the buffer and the run flags come after the wait.
+  // reads constant tables only; the buffer comes after the wait.
   grid_dependency_wait();
-  if (a.active && !a.active[run]) return;
   if (tid == 0)
     for (int d = 0; d < kEdgeDepth && d < kc; ++d) issue(d, d);
   mbar_wait(bars, 0, a.err, kErrEdgeRing);
@@ -428,7 +428,7 @@ struct StageArgs {
   T* divout;                // MODE 4/5: compact divergence [face][k][j][i]
   const T* force;           // FORCE: this step's forcing field [face][j][i] (v_r equation)
   const T* force_r;         // FORCE: its radial factor [nr]
-  const int* active;
+  const int* runs;          // stored run of each launched run index, or nullptr
   int* err;
   Geom g;
   T dt, alpha, beta, inv_dxi;
@@ -470,7 +470,9 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __
   const int n = g.n, nr = g.nr;
   const int tiles_x = n / TX;
   const int i0 = (blockIdx.x % tiles_x) * TX, j0 = (blockIdx.x / tiles_x) * TY;
-  const int run = blockIdx.z / g.nface, face = g.face0 + blockIdx.z % g.nface;
+  // the run map is written before the launches that use it and constant during them
+  const int zr = blockIdx.z / g.nface;
+  const int run = a.runs ? a.runs[zr] : zr, face = g.face0 + blockIdx.z % g.nface;
   const int kb = blockIdx.y * a.kchunk;
   if (kb >= nr) return;
   const int ke = min(nr, kb + a.kchunk);
@@ -526,10 +528,8 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __
   }
   __syncthreads();
   // The previous kernel may still be finishing (programmatic launch): everything above
-  // reads constant tables only; the state, the run flags and the source term come after
-  // the wait.
+  // reads constant tables only; the state and the source term come after the wait.
   grid_dependency_wait();
-  if (a.active && !a.active[run]) return;
   // producer state (thread 0 only)
   int m_issued = m_lo, slot_issue = 0;
   if (tid == 0) {
@@ -751,7 +751,7 @@ template <typename T>
 struct FilterArgs {
   CUtensorMap mP;           // input buffer, box (TX+8) x (TY+6)
   T* qout;
-  const int* active;
+  const int* runs;          // stored run of each launched run index, or nullptr
   int* err;
   Geom g;
   int whole;                // CTAs 0 .. whole-1 filter one (tile, field, face, run) unit each
@@ -797,7 +797,7 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) filter_kernel(const _
   const int i0 = (tile % tiles_x) * TX, j0 = (tile / tiles_x) * TY;
   const int s = rest % g.nf;                 // stored field
   const int rz = rest / g.nf;
-  const int run = rz / g.nface, face = g.face0 + rz % g.nface;
+  const int run = a.runs ? a.runs[rz / g.nface] : rz / g.nface, face = g.face0 + rz % g.nface;
   const int cx = threadIdx.x, ty = threadIdx.y, tid = ty * NT + cx;
   constexpr int PW = TX + 8;
   const int z0 = ((run * 6 + face) * g.nf + s) * nr;
@@ -812,10 +812,9 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) filter_kernel(const _
     mbar_fence_init();
   }
   __syncthreads();
-  // The previous kernel may still be finishing (programmatic launch): the input and the
-  // run flags are read only after the wait.
+  // The previous kernel may still be finishing (programmatic launch): the input is read
+  // only after the wait.
   grid_dependency_wait();
-  if (a.active && !a.active[run]) return;
   if (tid == 0)
     for (int k = ks; k < min(ks + kFiltRing, ke); ++k) issue(k, k - ks);
   T* out = a.qout + g.vol(run, face, s) + g.at(0, j0 + ty, i0 + V * cx);
@@ -1135,14 +1134,5 @@ __global__ void reduce_final_kernel(const double* part, int nblocks, double* out
     for (int m = 0; m < 5; ++m) out[m] = red[m][0];
 }
 
-// Batched runs: per-step activity flags and step counters (kernel boundaries order them).
-__global__ void batch_tick_kernel(const int* target, const int* done, int* active, int nruns) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r < nruns) active[r] = done[r] < target[r] ? 1 : 0;
-}
-__global__ void batch_tock_kernel(const int* active, int* done, int nruns) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r < nruns) done[r] += active[r];
-}
 
 }  // namespace solar

@@ -104,14 +104,13 @@ struct solar_ctx {
   double* stage64 = nullptr;   // one (face, field) compact FP64 volume
   double* part = nullptr;      // reduction partials
   double* red_out = nullptr;   // reduction result (device)
-  int* active = nullptr;       // batched runs
-  int* target = nullptr;
-  int* done = nullptr;
+  int* run_order = nullptr;    // batched runs: stored runs, most steps first
+  int run_count = 0;           // runs in the launched grids while a run map is in use
   int* err = nullptr;          // device error word (bounded waits that gave up)
   DevTables dt;
   int tile_x = 32, tile_y = 8, kchunk = 0, edge_kchunk = 16;
   cudaGraphExec_t step_graph = nullptr;
-  cudaGraphExec_t batch_graph = nullptr;
+  std::vector<cudaGraphExec_t> batch_graphs;   // batched step graph per number of live runs
   cudaEvent_t ev[8] = {};
   AdjBuffers adj;
   int forcing = 0;             // SOLAR_FORCING_*
@@ -183,6 +182,9 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   return fn;
 }
 
+// Runs covered by a launch: all of them, or the first run_count entries of a run map.
+static int launched_runs(const solar_ctx* c, const int* runs) { return runs ? c->run_count : c->g.nruns; }
+
 // Launch with programmatic stream serialization: the kernel starts as the previous kernel
 // in the stream retires its last CTAs, does its constant-table prologue, and waits on the
 // device (griddepcontrol.wait) before it touches anything that kernel wrote.  Used for the
@@ -252,13 +254,13 @@ static int edge_windows(solar_ctx* c) {
 }
 
 template <typename T>
-static int launch_edge(solar_ctx* c, void* buf, int mode, const int* active) {
+static int launch_edge(solar_ctx* c, void* buf, int mode, const int* runs) {
   EdgeArgs<T> a;
   a.q = (T*)buf;
   a.ew = (const T*)c->dt.ew;
   a.eg = (const T*)c->dt.eg;
   a.s0t = c->dt.s0t;
-  a.active = active;
+  a.runs = runs;
   a.win = (const int2*)c->dt.ewin;
   a.g = c->g;
   a.mode = mode;
@@ -267,7 +269,8 @@ static int launch_edge(solar_ctx* c, void* buf, int mode, const int* active) {
   a.sp = c->dt.ewin_sp;
   a.ngroups = mode == 1 ? (c->g.nf + 1) / 2 : 2;
   // About one wave of resident CTAs, each marching at least 4 planes.
-  const long long per_chunk = 4LL * c->g.nface * a.ngroups * a.nseg * c->g.nruns;
+  const int nrl = launched_runs(c, runs);
+  const long long per_chunk = 4LL * c->g.nface * a.ngroups * a.nseg * nrl;
   const long long slots = (long long)c->nsm * EdgeMinBlocks<T>::value;
   const long long nch = std::max<long long>(1, slots / per_chunk);
   a.kchunk = std::max<int>(4, (int)((c->g.nr + nch - 1) / nch));
@@ -283,7 +286,7 @@ static int launch_edge(solar_ctx* c, void* buf, int mode, const int* active) {
     CK(cudaFuncSetAttribute(edge_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     attr_set = true;
   }
-  dim3 grid((c->g.nr + a.kchunk - 1) / a.kchunk, 4 * c->g.nface * a.ngroups * a.nseg, c->g.nruns);
+  dim3 grid((c->g.nr + a.kchunk - 1) / a.kchunk, 4 * c->g.nface * a.ngroups * a.nseg, nrl);
   CK(launch_pdl(edge_kernel<T>, grid, dim3(3 * a.ts), smem, c->stream, a));
   return SOLAR_OK;
 }
@@ -302,7 +305,7 @@ static int launch_stage_t(solar_ctx* c, StageArgs<T>& a, const void* qin) {
     attr_set = true;
   }
   const int nchunks = (c->g.nr + a.kchunk - 1) / a.kchunk;
-  dim3 grid((c->g.n / TX) * (c->g.n / TY), nchunks, c->g.nruns * c->g.nface);
+  dim3 grid((c->g.n / TX) * (c->g.n / TY), nchunks, launched_runs(c, a.runs) * c->g.nface);
   CK(launch_pdl(stage_kernel<T, TX, TY, MODE, HAS_RHO, FORCE>, grid, dim3(TX / Vec16<T>::V, TY), L::TOTAL, c->stream, a));
   return SOLAR_OK;
 }
@@ -342,7 +345,7 @@ static void default_tile(int n, bool fp32, int* tx, int* ty) {
 
 template <typename T>
 static int launch_stage(solar_ctx* c, const void* qin, void* qout, int mode, int stage,
-                        const int* active, void* divout = nullptr) {
+                        const int* runs, void* divout = nullptr) {
   StageArgs<T> a;
   a.divout = (T*)divout;
   const bool forced = c->forcing && mode != 3;     // every mode but the gradient/divergence operator
@@ -353,7 +356,7 @@ static int launch_stage(solar_ctx* c, const void* qin, void* qout, int mode, int
   a.rad = (const T*)c->dt.rad;
   a.met = (const T*)c->dt.met;
   a.c2 = (const T*)c->dt.c2;
-  a.active = active;
+  a.runs = runs;
   a.err = c->err;
   a.g = c->g;
   a.dt = (T)c->desc.dt;
@@ -371,12 +374,12 @@ static int launch_stage(solar_ctx* c, const void* qin, void* qout, int mode, int
 }
 
 template <typename T, int TX, int TY>
-static int launch_filter_t(solar_ctx* c, const void* qin, void* qout, const int* active) {
+static int launch_filter_t(solar_ctx* c, const void* qin, void* qout, const int* runs) {
   using L = FilterLayout<T, TX, TY>;
   FilterArgs<T> a;
   if (!make_map(c, qin, TX + 8, TY + 6, &a.mP)) return fail(SOLAR_ERR_CUDA, "cuTensorMapEncodeTiled failed");
   a.qout = (T*)qout;
-  a.active = active;
+  a.runs = runs;
   a.err = c->err;
   a.g = c->g;
   static bool attr_set = false;
@@ -390,7 +393,7 @@ static int launch_filter_t(solar_ctx* c, const void* qin, void* qout, const int*
   }
   // Whole-column CTAs for every full wave; the units of a last, partial wave are cut into
   // radial chunks (at least 11 planes each) so that they fill one wave.
-  const long long units = (long long)(c->g.n / TX) * (c->g.n / TY) * c->g.nf * c->g.nruns * c->g.nface;
+  const long long units = (long long)(c->g.n / TX) * (c->g.n / TY) * c->g.nf * launched_runs(c, runs) * c->g.nface;
   const long long slots = (long long)c->nsm * resident;
   const long long tail = units % slots;
   a.whole = (int)units;
@@ -408,9 +411,9 @@ static int launch_filter_t(solar_ctx* c, const void* qin, void* qout, const int*
 }
 
 template <typename T>
-static int launch_filter(solar_ctx* c, const void* qin, void* qout, const int* active) {
-  if (c->g.n % 32 == 0) return launch_filter_t<T, 32, 16>(c, qin, qout, active);
-  return launch_filter_t<T, 16, 16>(c, qin, qout, active);
+static int launch_filter(solar_ctx* c, const void* qin, void* qout, const int* runs) {
+  if (c->g.n % 32 == 0) return launch_filter_t<T, 32, 16>(c, qin, qout, runs);
+  return launch_filter_t<T, 16, 16>(c, qin, qout, runs);
 }
 
 static int force_begin(solar_ctx* c);   // forcing.cuh: this step's source field
@@ -419,7 +422,7 @@ static int force_end(solar_ctx* c);     // forcing.cuh: time += dt, step += 1
 // One full time step (timestep.f90:61-82) on every run.  With ev != nullptr each kernel
 // is bracketed by events: ev_pairs[kind] accumulates into times[kind].
 template <typename T>
-static int enqueue_step(solar_ctx* c, const int* active, std::vector<cudaEvent_t>* evs) {
+static int enqueue_step(solar_ctx* c, const int* runs, std::vector<cudaEvent_t>* evs) {
   void* bufs[2] = {c->A, c->B};
   int cur = 0, rc;
   if ((rc = force_begin(c))) return rc;
@@ -432,22 +435,22 @@ static int enqueue_step(solar_ctx* c, const int* active, std::vector<cudaEvent_t
   };
   for (int s = 0; s < 5; ++s) {
     mark();
-    if ((rc = launch_edge<T>(c, bufs[cur], 0, active))) return rc;
+    if ((rc = launch_edge<T>(c, bufs[cur], 0, runs))) return rc;
     mark();
-    if ((rc = launch_stage<T>(c, bufs[cur], bufs[cur ^ 1], s == 0 ? 1 : 0, s, active))) return rc;
+    if ((rc = launch_stage<T>(c, bufs[cur], bufs[cur ^ 1], s == 0 ? 1 : 0, s, runs))) return rc;
     mark();
     cur ^= 1;
   }
   mark();
-  if ((rc = launch_edge<T>(c, bufs[cur], 1, active))) return rc;
+  if ((rc = launch_edge<T>(c, bufs[cur], 1, runs))) return rc;
   mark();
-  if ((rc = launch_filter<T>(c, bufs[cur], bufs[cur ^ 1], active))) return rc;
+  if ((rc = launch_filter<T>(c, bufs[cur], bufs[cur ^ 1], runs))) return rc;
   mark();
   return force_end(c);
 }
 
-static int enqueue_step_any(solar_ctx* c, const int* active, std::vector<cudaEvent_t>* evs) {
-  return c->fp32 ? enqueue_step<float>(c, active, evs) : enqueue_step<double>(c, active, evs);
+static int enqueue_step_any(solar_ctx* c, const int* runs, std::vector<cudaEvent_t>* evs) {
+  return c->fp32 ? enqueue_step<float>(c, runs, evs) : enqueue_step<double>(c, runs, evs);
 }
 
 // Device error word: set by a kernel whose bounded wait gave up.
@@ -476,20 +479,26 @@ static int capture_step_graph(solar_ctx* c) {
   return SOLAR_OK;
 }
 
-static int capture_batch_graph(solar_ctx* c) {
-  if (c->batch_graph) return SOLAR_OK;
-  const int R = c->g.nruns;
+// Step graph over the first `live` runs of run_order (the runs with the most steps left).
+static int capture_batch_graph(solar_ctx* c, int live) {
+  if ((int)c->batch_graphs.size() < c->g.nruns + 1) c->batch_graphs.resize(c->g.nruns + 1, nullptr);
+  if (c->batch_graphs[live]) return SOLAR_OK;
   cudaGraph_t graph;
+  c->run_count = live;
   CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-  batch_tick_kernel<<<(R + 127) / 128, 128, 0, c->stream>>>(c->target, c->done, c->active, R);
-  int rc = enqueue_step_any(c, c->active, nullptr);
-  batch_tock_kernel<<<(R + 127) / 128, 128, 0, c->stream>>>(c->active, c->done, R);
+  int rc = enqueue_step_any(c, c->run_order, nullptr);
   cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
+  c->run_count = 0;
   if (rc) return rc;
   CK(ce);
-  CK(cudaGraphInstantiate(&c->batch_graph, graph, 0));
+  CK(cudaGraphInstantiate(&c->batch_graphs[live], graph, 0));
   CK(cudaGraphDestroy(graph));
   return SOLAR_OK;
+}
+
+static void drop_batch_graphs(solar_ctx* c) {
+  for (auto& gx : c->batch_graphs)
+    if (gx) { cudaGraphExecDestroy(gx); gx = nullptr; }
 }
 
 // ---------------------------------------------------------------- transfers
@@ -624,8 +633,8 @@ int solar_gpu_finalize(solar_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
-  if (c->batch_graph) cudaGraphExecDestroy(c->batch_graph);
-  void* ptrs[] = {c->A, c->B, c->W, c->stage64, c->part, c->red_out, c->active, c->target, c->done,
+  drop_batch_graphs(c);
+  void* ptrs[] = {c->A, c->B, c->W, c->stage64, c->part, c->red_out, c->run_order,
                   c->err, c->dt.rad, c->dt.met, c->dt.ew, c->dt.eg, c->dt.egc, c->dt.s0t, c->dt.ewin, c->dt.c2,
                   c->dt.rad64, c->dt.vol2, c->dt.drw, c->dt.c2_64, c->dt.tanx, c->dt.gr};
   for (void* p : ptrs)
@@ -715,9 +724,7 @@ int solar_gpu_init(const solar_desc* d, solar_ctx** out) {
   TRYC(cudaMalloc((void**)&c->stage64, (size_t)vol_compact(c) * sizeof(double)));
   TRYC(cudaMalloc((void**)&c->part, (size_t)6 * g.nr * 5 * sizeof(double)));
   TRYC(cudaMalloc((void**)&c->red_out, 5 * sizeof(double)));
-  TRYC(cudaMalloc((void**)&c->active, g.nruns * sizeof(int)));
-  TRYC(cudaMalloc((void**)&c->target, g.nruns * sizeof(int)));
-  TRYC(cudaMalloc((void**)&c->done, g.nruns * sizeof(int)));
+  TRYC(cudaMalloc((void**)&c->run_order, g.nruns * sizeof(int)));
   TRY(upload_constants());
   if (c->fp32) TRY(upload_tables<float>(c));
   else TRY(upload_tables<double>(c));
@@ -813,16 +820,28 @@ static int rk4_runs_impl(solar_ctx* c, const int* nsteps_per_run, double* ms) {
   if (rc) return rc;
   if (!nsteps_per_run) return fail(SOLAR_ERR_ARG, "null step counts");
   const int R = c->g.nruns;
-  int maxs = 0;
-  for (int r = 0; r < R; ++r) {
+  for (int r = 0; r < R; ++r)
     if (nsteps_per_run[r] < 0) return fail(SOLAR_ERR_ARG, "negative step count");
-    maxs = std::max(maxs, nsteps_per_run[r]);
+  // Runs ordered by step count, most first: while s steps are done, the live runs are the
+  // first (count of runs with more than s steps) entries, so each stretch of steps with the
+  // same live count replays one graph whose grids cover exactly those runs.
+  std::vector<int> order(R);
+  for (int r = 0; r < R; ++r) order[r] = r;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int x, int y) { return nsteps_per_run[x] > nsteps_per_run[y]; });
+  CK(cudaMemcpyAsync(c->run_order, order.data(), R * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));   // the host copy of `order` goes out of scope below
+  std::vector<std::pair<int, int>> stretches;   // (live runs, steps)
+  int done = 0;
+  for (int live = R; live > 0; --live) {
+    const int until = nsteps_per_run[order[live - 1]];
+    if (until > done) { stretches.push_back({live, until - done}); done = until; }
   }
-  CK(cudaMemcpyAsync(c->target, nsteps_per_run, R * sizeof(int), cudaMemcpyHostToDevice, c->stream));
-  CK(cudaMemsetAsync(c->done, 0, R * sizeof(int), c->stream));
-  if ((rc = capture_batch_graph(c))) return rc;
+  for (const auto& st : stretches)
+    if ((rc = capture_batch_graph(c, st.first))) return rc;
   CK(cudaEventRecord(c->ev[0], c->stream));
-  for (int s = 0; s < maxs; ++s) CK(cudaGraphLaunch(c->batch_graph, c->stream));
+  for (const auto& st : stretches)
+    for (int s = 0; s < st.second; ++s) CK(cudaGraphLaunch(c->batch_graphs[st.first], c->stream));
   CK(cudaEventRecord(c->ev[1], c->stream));
   CK(cudaStreamSynchronize(c->stream));
   if (ms) {

@@ -84,7 +84,7 @@ int solar_gpu_set_owned_zones(solar_ctx* c, int zone0, int nzones) {
   c->g.nface = nzones;
   // captured graphs hold the old launch shapes
   if (c->step_graph) { cudaGraphExecDestroy(c->step_graph); c->step_graph = nullptr; }
-  if (c->batch_graph) { cudaGraphExecDestroy(c->batch_graph); c->batch_graph = nullptr; }
+  drop_batch_graphs(c);
   return SOLAR_OK;
 }
 
