@@ -409,7 +409,7 @@ enum { mD = 0, mXYD, mC, mXYC, mDivX, mDivY, mTX, mTY, mVol, mCount };
 // grad_r, div) into the v_xi, v_eta, v_r, p slots of qout.  MODE 4 / 5: MODE 1 / 0 that
 // also store the divergence of the stage input (compact, run 0) into divout -- the
 // forward recomputation of the adjoint.
-constexpr int kLead = 7;
+constexpr int kLead = 8;
 // tile-ring depth: plane k is computed while planes k+1, k+2 are in flight
 template <typename T> struct TileRing { static constexpr int value = 3; };
 
