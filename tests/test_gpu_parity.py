@@ -260,6 +260,25 @@ def test_batched_uneven_runs_match_single_runs(c1_small):
             assert np.array_equal(s.get_state(), got[r]), r
 
 
+def test_batched_runs_twice_reorders_live_runs(c1_small):
+    """Two batched calls with different step counts: the second reorders the runs, reuses
+    the graphs kept per live-run count, and still matches each run advanced on its own."""
+    srcs = [configs.Source((0.0, 0.0, 0.75), 0.05, 1.0), configs.Source((0.75, 0.0, 0.0), 0.04, 0.5),
+            configs.Source((0.0, -0.7, 0.2), 0.06, 2.0)]
+    first, second = [2, 5, 3], [4, 1, 4]
+    with Solver(c1_small, nruns=3) as b:
+        for r, src in enumerate(srcs):
+            b.init_sources([src], run=r)
+        b.rk4_runs(first)
+        b.rk4_runs(second)
+        got = [b.get_state(r) for r in range(3)]
+    with Solver(c1_small) as s:
+        for r, src in enumerate(srcs):
+            s.init_sources([src])
+            s.rk4(first[r] + second[r])
+            assert np.array_equal(s.get_state(), got[r]), r
+
+
 def test_norm_and_diag(oracle_mod, c1_small):
     o = oracle_mod.Oracle(c1_small)
     q = smooth_state(o, 6)
