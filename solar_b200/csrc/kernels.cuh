@@ -177,7 +177,7 @@ struct EdgeArgs {
 // shared memory and one thread per row writes the row's whole 32-byte sector (ghost
 // columns plus the padding next to them): writing 12 of 32 bytes would make the L2 read
 // the sector back from DRAM to merge it.
-constexpr int kEdgeDepth = 4;               // planes in flight ahead of the computed one
+constexpr int kEdgeDepth = 3;               // planes in flight ahead of the computed one
 constexpr int kEdgeRing = kEdgeDepth + 2;   // a slot is refilled two planes after its last read
 
 // Shared memory of one CTA in bytes: staging ring (two fields of 4 * sp values per slot),
