@@ -692,7 +692,11 @@ int solar_gpu_init(const solar_desc* d, solar_ctx** out) {
   {
     const int tx = c->tile_x, ty = c->tile_y;
     const bool known = (tx == 16 && ty == 16) || (tx == 32 && (ty == 8 || ty == 16)) || (tx == 64 && ty == 8);
-    if (!known || g.n % tx || g.n % ty) { delete c; return fail(SOLAR_ERR_ARG, "unsupported stage tile %d x %d for nx %d", tx, ty, g.n); }
+    if (!known || g.n % tx || g.n % ty) {
+      const int nx = g.n;          // g refers into c
+      delete c;
+      return fail(SOLAR_ERR_ARG, "unsupported stage tile %d x %d for nx %d", tx, ty, nx);
+    }
   }
   if (d->kchunk > 0) c->kchunk = d->kchunk;
   else {
