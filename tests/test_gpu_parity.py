@@ -296,3 +296,15 @@ def test_bad_run_index_raises(c1_small):
     with Solver(c1_small) as s:
         with pytest.raises(SolarError):
             s.get_state(run=3)
+
+
+def test_unsupported_tile_is_rejected(c1_small):
+    """A stage tile the library does not build, or one that does not divide nx, is refused at
+    set-up with SOLAR_ERR_ARG and a message naming it; a valid context still opens after it."""
+    from solar_b200._lib import SolarError
+    for tile in ((48, 8, 0), (64, 8, 0)):          # unknown shape; 64 does not divide nx = 32
+        with pytest.raises(SolarError, match="unsupported stage tile"):
+            Solver(c1_small, tile=tile)
+    with Solver(c1_small, tile=(16, 16, 0)) as s:
+        s.init_sources()
+        assert s.norm(5) > 0
