@@ -71,7 +71,13 @@ typedef struct solar_desc {
   int fix_reversed_rotation; /* 0 (default) = reference arithmetic.  1 = evaluate the
                             receiver-frame rotation of the eight reversed vector strips
                             (transform.f90:184-274) at the receiver's mirrored edge index  */
-  int tile_x, tile_y, kchunk; /* stage-kernel tile; 0 = tuned default                     */
+  int tile_x, tile_y, kchunk; /* stage-kernel tile (16x16, 32x8, 32x16 or 64x8) and radial
+                                planes per CTA; 0 = default: 64x8 when nx is a multiple of
+                                64, else 32x16 (float) / 32x8 (double), 16x16 when nx is
+                                not a multiple of 32; nr/3 (float) or nr/6 (double) planes,
+                                clamped to 16..64 (finer when that would not fill one wave
+                                of two CTAs per SM).  solar_b200/autotune.py measures the
+                                best for a workload.                                         */
 } solar_desc;
 
 /* Fill *d with the reference's defaults (sizes 0, FP64, 5 fields, 1 run, device 0,
