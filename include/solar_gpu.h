@@ -60,7 +60,7 @@ typedef struct solar_desc {
                       so the host sets it                                                  */
   const double* model;   /* nr x 8 'solar_model' rows, row-major (r/R, c, rho, p, T, g,
                             Gamma, unused), normalised here as SOLAR_DATA does
-                            (ic_acoustic_wave.f90:236-271)                                  */
+                            (ic_acoustic_wave.f90:73-108)                                   */
   const double* c2_3d;   /* optional six-zone field of c^2 replacing the radial c^2 (a 3-D
                             sound-speed perturbation); NULL = radial background            */
   double sponge_amp;     /* a_sponge = 0.1   (sponge.f90:20)                               */
@@ -149,12 +149,40 @@ int solar_gpu_norm(solar_ctx* c, int run, int field, double* out);
  * another runtime, or a per-step diagnostic hook that must not trigger the device-wide
  * synchronisation of cudaMalloc/cudaFree).  No counterpart in the reference: it has no
  * device.  Allocates nothing: its scratch is a fixed 96 KiB device array inside the
- * library, so nr <= 2048 (larger grids return SOLAR_ERR_ARG).  d_out is one device double;
- * the call only enqueues work on `stream` (a cudaStream_t, NULL = legacy default stream).
- * The first call on a device resolves the scratch address and should come before any
+ * library, so nr <= 2048 and nx * nx <= INT_MAX (larger grids return SOLAR_ERR_ARG before
+ * any launch).  d_out is one device double; the call only enqueues work on `stream` (a
+ * cudaStream_t, NULL = legacy default stream).  The first call in each CUDA context
+ * resolves the scratch address (again after a cudaDeviceReset) and should come before any
  * stream capture.  Calls whose kernels overlap on the same device race on the shared
  * scratch. */
 int solar_gpu_norm_noalloc(const double* d_field, int nx, int nr, double* d_out, void* stream);
+
+/* cube.f90:71-79 loop body without the host waits: nsteps calls of RK4 (as solar_gpu_rk4)
+ * and after each the norm (auxiliary.f90:100-125, as solar_gpu_norm) of field m (1..5) of
+ * one run.  norms[s] = the norm after step s+1.  The per-step sums stay on the device and
+ * are read back once at the end, so the host does not wait on the GPU between steps. */
+int solar_gpu_rk4_norms(solar_ctx* c, int run, int field, int nsteps, double* norms);
+
+/* NaN/Inf watchdog.  No counterpart in the reference, which only prints norm(v_r) after
+ * each step (cube.f90:77).  With every > 0, solar_gpu_rk4, solar_gpu_rk4_runs,
+ * solar_gpu_rk4_norms, solar_gpu_time_rk4 and solar_gpu_step_phase scan the state buffer
+ * for non-finite values after every `every`-th step of the context (one read of the state,
+ * enqueued without a host wait); the call then returns SOLAR_ERR_NAN and
+ * solar_gpu_last_error names the first step (counted over the context's life) at which a
+ * non-finite value was seen.  every = 0 (the default) switches it off. */
+int solar_gpu_set_watchdog(solar_ctx* c, int every);
+
+/* Failure-detection test hook.  No counterpart in the reference.  Every wait of a
+ * streaming kernel on its shared-memory load ring is bounded (one second); a kernel whose
+ * wait gives up stops issuing loads, waits (bounded) for the loads it issued, exits, and
+ * the call returns SOLAR_ERR_TIMEOUT.  With kernels != 0 the named kernels issue no loads
+ * at all and wait at most wait_us microseconds, so their first wait gives up with nothing
+ * in flight; kernels = 0 restores normal operation.  Captured step graphs are rebuilt. */
+#define SOLAR_KERNEL_EDGE 1
+#define SOLAR_KERNEL_STAGE 2
+#define SOLAR_KERNEL_FILTER 4
+#define SOLAR_KERNEL_ADJ_STAGE 8
+int solar_gpu_inject_wait_timeout(solar_ctx* c, int kernels, int wait_us);
 
 /* FP64 diagnostics of one run: out[0] = acoustic energy
  * 1/2 sum (rho0 |v|^2 + p^2 / (rho0 c^2)) dV, out[1] = sum rho dV, out[2] = max |p|,

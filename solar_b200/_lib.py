@@ -25,6 +25,10 @@ SOLAR_FORCING_ANALYTIC = 1
 SOLAR_FORCING_SAMPLES = 2
 SOLAR_FP64 = 0
 SOLAR_FP32 = 1
+SOLAR_KERNEL_EDGE = 1
+SOLAR_KERNEL_STAGE = 2
+SOLAR_KERNEL_FILTER = 4
+SOLAR_KERNEL_ADJ_STAGE = 8
 
 
 class SolarError(RuntimeError):
@@ -68,6 +72,9 @@ EXPORTS = {
     "solar_gpu_curl": [_P, _D, _D, _D, _D, _D, _D],
     "solar_gpu_norm": [_P, ctypes.c_int, ctypes.c_int, _D],
     "solar_gpu_norm_noalloc": [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
+    "solar_gpu_rk4_norms": [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int, _D],
+    "solar_gpu_set_watchdog": [_P, ctypes.c_int],
+    "solar_gpu_inject_wait_timeout": [_P, ctypes.c_int, ctypes.c_int],
     "solar_gpu_diag": [_P, ctypes.c_int, _D],
     "solar_gpu_time_rk4": [_P, ctypes.c_int, ctypes.c_int, _D],
     "solar_gpu_synchronize": [_P],

@@ -52,7 +52,7 @@ struct AdjStageArgs {
   double* grad;
   const T* rad;
   const T* met;
-  int* err;
+  WaitCtl wc;         // error word and bound of the ring waits
   Geom g;
   T alpha, beta, dt, inv_dxi;
   int keep, kchunk;
@@ -147,8 +147,10 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const __grid_cons
     mbar_fence_init();
   }
   __syncthreads();
-  int m_issued = m_lo;
-  if (tid == 0) {
+  // planes [m_lo, m_issued) have loads issued; thread 0 has seen planes [m_lo, m_seen) land
+  int m_issued = m_lo, m_seen = m_lo;
+  const bool loads = !a.wc.no_loads;
+  if (tid == 0 && loads) {
     tma_prefetch_desc(&a.mBq);
     tma_prefetch_desc(&a.mBw);
     for (int q = 0; q < L::RING && m_issued <= m_hi; ++q, ++m_issued) issue(m_issued, q);
@@ -161,7 +163,7 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const __grid_cons
   for (int q = 0; q < 4; ++q) { pp[q] = T(0); pv[q] = T(0); }
   int slot = 0;
   uint32_t phase = 0;
-  bool ok = true;
+  bool ok = true, failed = false;
   const int bo = (ty + 3) * PW + tx + 4;           // own point in a box
   const int to = ty * TX + tx;                     // own point in a tile
   for (int m = kb - 3; m <= ke + 2; ++m) {
@@ -179,7 +181,10 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const __grid_cons
       const T hc2 = (do_halo && a.c2) ? __ldg(a.c2 + plane_c2 + hq2) : T(0);
       const T invr = __ldg(rad + rInvR * nr + m), inv_rho0 = __ldg(rad + rInvRho0 * nr + m);
       const T rho0 = __ldg(rad + rRho0 * nr + m), c2r = __ldg(rad + rC2Rho0 * nr + m);
-      ok &= mbar_wait(&bars[slot], phase, a.err, kErrAdjointRing);
+      if (ok) {
+        ok = mbar_wait(&bars[slot], phase, a.wc, kErrAdjointRing);
+        if (ok) m_seen = m + 1;
+      }
       const T* sb = reinterpret_cast<const T*>(slot_base(slot));
       constexpr int PBs = (int)(L::P_BYTES / sizeof(T)), OBs = (int)(L::O_BYTES / sizeof(T));
       T lqv[5], lwv[5];
@@ -327,15 +332,13 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const __grid_cons
     }
     if (real) {
       // every thread is done with this slot (and with the X/Y arrays): refill it
-      if (__syncthreads_or(!ok)) break;
-      if (tid == 0 && m_issued <= m_hi) issue(m_issued++, slot);
+      if (__syncthreads_or(!ok)) { failed = true; break; }
+      if (tid == 0 && loads && m_issued <= m_hi) issue(m_issued++, slot);
       if (++slot == L::RING) { slot = 0; phase ^= 1; }
     }
   }
-  if (!ok && tid == 0) {
-    // a wait gave up: give copies still in flight a bounded time to land before exit
-    for (int q = 0; q < 1000; ++q) __nanosleep(1000);
-  }
+  // a wait gave up: wait (bounded) for the loads still in flight before the CTA exits
+  if (failed && tid == 0) mbar_drain(bars, L::RING, m_lo, m_seen, m_issued, a.wc.ns);
 }
 
 // The one-sided radial rows 1, 2 (onto planes 0..6) and nr-3, nr-2 (onto planes nr-7..nr-1)

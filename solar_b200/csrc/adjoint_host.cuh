@@ -82,7 +82,7 @@ static AdjStageArgs<T> adj_args(solar_ctx* c, double dt) {
   a.inv_dxi = (T)(1.0 / c->ht.dxi);
   a.keep = 0;
   a.kchunk = 0;
-  a.err = c->err;
+  a.wc = wait_ctl(c, kInjAdjStage);
   return a;
 }
 
@@ -121,7 +121,7 @@ static int enqueue_rhs_adjoint(solar_ctx* c, AdjStageArgs<T> a) {
   a.lout = (T*)b.T1;
   a.lwout = (T*)b.T2;
   a.rb = (T*)b.rb;
-  a.err = c->err;
+  a.wc = wait_ctl(c, kInjAdjStage);
   if ((long long)g.nf * g.vs >= (1LL << 31))     // the kernel indexes one face's fields in 32 bits
     return fail(SOLAR_ERR_ARG, "grid too large for the adjoint (%lld values per face)", (long long)g.nf * g.vs);
   int rc = (g.n % 32 == 0) ? launch_adj_stage<T, 32, 8>(c, a) : launch_adj_stage<T, 16, 16>(c, a);
@@ -409,7 +409,8 @@ int solar_gpu_rhs_adjoint(solar_ctx* c, const double* mu, double* out) {
   rc = c->fp32 ? enqueue_rhs_adjoint<float>(c, adj_args<float>(c, 1.0))
                : enqueue_rhs_adjoint<double>(c, adj_args<double>(c, 1.0));
   if (rc) return rc;
-  return download_fields(c, c->adj.L, 0, out, 5, kAllFields, 5);
+  if ((rc = download_fields(c, c->adj.L, 0, out, 5, kAllFields, 5))) return rc;
+  return check_device_error(c);
 }
 
 int solar_gpu_filter_adjoint(solar_ctx* c, const double* lam, double* out) {
@@ -420,7 +421,8 @@ int solar_gpu_filter_adjoint(solar_ctx* c, const double* lam, double* out) {
   if ((rc = upload_fields(c, c->adj.L, 0, lam, 5, kAllFields, 5))) return rc;
   rc = c->fp32 ? enqueue_filter_adjoint<float>(c) : enqueue_filter_adjoint<double>(c);
   if (rc) return rc;
-  return download_fields(c, c->adj.L, 0, out, 5, kAllFields, 5);
+  if ((rc = download_fields(c, c->adj.L, 0, out, 5, kAllFields, 5))) return rc;
+  return check_device_error(c);
 }
 
 int solar_gpu_rk4_adjoint(solar_ctx* c, int nsteps, const double* lam_in, double* lam_out) {
@@ -434,7 +436,8 @@ int solar_gpu_rk4_adjoint(solar_ctx* c, int nsteps, const double* lam_in, double
     rc = c->fp32 ? enqueue_step_adjoint<float>(c, nullptr, nullptr) : enqueue_step_adjoint<double>(c, nullptr, nullptr);
     if (rc) return rc;
   }
-  return download_fields(c, c->adj.L, 0, lam_out, 5, kAllFields, 5);
+  if ((rc = download_fields(c, c->adj.L, 0, lam_out, 5, kAllFields, 5))) return rc;
+  return check_device_error(c);
 }
 
 }  // extern "C"

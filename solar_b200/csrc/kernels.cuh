@@ -157,7 +157,7 @@ struct EdgeArgs {
   int ts, nseg;             // positions per segment, segments per edge
   int ngroups;              // field groups per edge: 2 in mode 0, ceil(nf / 2) in mode 1
   int sp;                   // staged positions per line (window capacity, a multiple of 8)
-  int* err;                 // device error word (a bounded wait gave up)
+  WaitCtl wc;               // error word and bound of the ring waits
 };
 
 // One CTA per (run, receiving face and edge, field group, segment of ts positions along
@@ -321,20 +321,25 @@ __global__ void __launch_bounds__(384, (EdgeMinBlocks<T>::value)) edge_kernel(co
   // The previous kernel may still be finishing (programmatic launch): everything above
   // reads constant tables only; the buffer comes after the wait.
   grid_dependency_wait();
-  if (tid == 0)
+  // A thread whose wait gives up stops waiting and thread 0 stops issuing; the CTA leaves
+  // the plane loop at the next barrier, and thread 0 waits for the planes it issued but did
+  // not see land before the CTA exits.  fail_at = the plane whose wait thread 0 gave up on.
+  if (tid == 0 && !a.wc.no_loads)
     for (int d = 0; d < kEdgeDepth && d < kc; ++d) issue(d, d);
-  mbar_wait(bars, 0, a.err, kErrEdgeRing);
+  bool ok = mbar_wait(bars, 0, a.wc, kErrEdgeRing), failed = false;
+  int fail_at = ok ? kc : 0;
   spread(0, 0);
   int rs = 0;                                            // ring slot of plane kk
   int ws = kEdgeDepth;                                   // ring slot of plane kk + kEdgeDepth
   int ns = 1;                                            // ring slot of plane kk + 1 ...
   uint32_t np = 0;                                       // ... and the parity of its phase
-  for (int kk = 0; kk < kc; ++kk) {
-    if (tid == 0 && kk + kEdgeDepth < kc) issue(kk + kEdgeDepth, ws);
+  int kk = 0;
+  for (; kk < kc; ++kk) {
+    if (tid == 0 && ok && !a.wc.no_loads && kk + kEdgeDepth < kc) issue(kk + kEdgeDepth, ws);
     ws = ws + 1 == kEdgeRing ? 0 : ws + 1;
     if (ns == 0) np ^= 1;
-    if (kk + 1 < kc) mbar_wait(bars + ns, np, a.err, kErrEdgeRing);
-    __syncthreads();
+    if (ok && kk + 1 < kc && !mbar_wait(bars + ns, np, a.wc, kErrEdgeRing)) { ok = false; fail_at = kk + 1; }
+    if (__syncthreads_or(!ok)) { failed = true; break; }
     if (kk > 0) sectors((kk - 1) & 1);
     if (kk + 1 < kc) spread(ns, (kk + 1) & 1);
     const T* b = (along_i ? sm + rs * SLOT : tb + (kk & 1) * 2 * FS) + boff;
@@ -377,6 +382,16 @@ __global__ void __launch_bounds__(384, (EdgeMinBlocks<T>::value)) edge_kernel(co
     }
     rs = ns;
     ns = ns + 1 == kEdgeRing ? 0 : ns + 1;
+  }
+  if (failed) {
+    // thread 0 issued planes [0, issued): up to kk + kEdgeDepth at the break, or only the
+    // first kEdgeDepth if its first wait gave up; it saw [0, seen) land
+    if (tid == 0 && !a.wc.no_loads) {
+      const int issued = min(fail_at == 0 ? kEdgeDepth : kk + kEdgeDepth + 1, kc);
+      const int seen = min(fail_at, min(kk + 2, kc));
+      mbar_drain(bars, kEdgeRing, 0, seen, issued, a.wc.ns);
+    }
+    return;
   }
   if (cols) {
     __syncthreads();
@@ -429,7 +444,7 @@ struct StageArgs {
   const T* force;           // FORCE: this step's forcing field [face][j][i] (v_r equation)
   const T* force_r;         // FORCE: its radial factor [nr]
   const int* runs;          // stored run of each launched run index, or nullptr
-  int* err;
+  WaitCtl wc;               // error word and bound of the ring waits
   Geom g;
   T dt, alpha, beta, inv_dxi;
   int kchunk;
@@ -530,9 +545,10 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __
   // The previous kernel may still be finishing (programmatic launch): everything above
   // reads constant tables only; the state and the source term come after the wait.
   grid_dependency_wait();
-  // producer state (thread 0 only)
+  // producer state (thread 0 only): lead planes [m_lo, m_issued) have loads issued
   int m_issued = m_lo, slot_issue = 0;
-  if (tid == 0) {
+  const bool loads = !a.wc.no_loads;
+  if (tid == 0 && loads) {
     tma_prefetch_desc(&a.mP);
     for (; m_issued <= min(m_lo + kLead - 1, m_hi); ++m_issued) {
       issue_lead(m_issued, slot_issue);
@@ -582,11 +598,17 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __
     for (int q = 0; q < V; ++q) { pw[s][q] = T(0); vw[s][q] = T(0); }
   int mq = m_lo, slot_q = 0, slot_k = (kb - m_lo) % kLead, slot_t = 0;
   uint32_t phase_q = 0, phase_t = 0;
-  bool ok = true;
-  for (int k = kb; k < ke; ++k) {
+  // A thread whose wait gives up stops waiting; the CTA leaves at the barrier that closes
+  // the iteration, and thread 0 waits for what it issued but did not see land before the
+  // CTA exits.  lead_fail = the lead plane whose wait thread 0 gave up on; tile_fail = its
+  // tile wait gave up.
+  bool ok = true, failed = false, tile_fail = false;
+  int lead_fail = 0x7fffffff;
+  int k = kb;
+  for (; k < ke; ++k) {
     const int ks = clampk(k);
     for (; mq <= ks + 6; ++mq) {
-      ok &= mbar_wait(&barL[slot_q], phase_q, a.err, kErrStageLead);
+      if (ok && !mbar_wait(&barL[slot_q], phase_q, a.wc, kErrStageLead)) { ok = false; lead_fail = mq; }
       const T* bp = reinterpret_cast<const T*>(lead(slot_q));
 #pragma unroll
       for (int s = 0; s < 6; ++s)
@@ -596,7 +618,7 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __
       ldv(reinterpret_cast<const T*>(lead(slot_q) + L::P_BYTES) + oc, vw[6]);
       if (++slot_q == kLead) { slot_q = 0; phase_q ^= 1; }
     }
-    ok &= mbar_wait(&barT[slot_t], phase_t, a.err, kErrStageTile);
+    if (ok && !mbar_wait(&barT[slot_t], phase_t, a.wc, kErrStageTile)) { ok = false; tile_fail = true; }
     const Rad rn = load_rad(min(k + 1, nr - 1));
     const T* sp = reinterpret_cast<const T*>(lead(slot_k));
     const unsigned char* tb = tile(slot_t);
@@ -694,7 +716,7 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __
       stv(outS[kVr] + kp, r_vr);
       stv(outS[kP] + kp, r_p);
     } else {
-      // BC_RHS (bc_acoustic_wave.f90:432-452) then SPONGE (sponge.f90:502-504)
+      // BC_RHS (bc_acoustic_wave.f90:14-34) then SPONGE (sponge.f90:40-50)
       const bool bc = (k == 0 || k == nr - 1);
       const T sig = rc.sig;
       const T dt = a.dt, alpha = a.alpha, beta = a.beta;
@@ -718,8 +740,8 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __
       update(kP, pv, r_p, true);
     }
     // every thread is done with lead plane k and tile plane k: refill their slots
-    if (__syncthreads_or(!ok)) break;
-    if (tid == 0) {
+    if (__syncthreads_or(!ok)) { failed = true; break; }
+    if (tid == 0 && loads) {
       if (k + kTile < ke) issue_tile(k + kTile, slot_t);
       for (; m_issued <= min(k + kLead, m_hi); ++m_issued) {
         issue_lead(m_issued, slot_issue);
@@ -730,9 +752,12 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __
     if (++slot_k == kLead) slot_k = 0;
     rc = rn;
   }
-  if (!ok && tid == 0) {
-    // a wait gave up: give copies still in flight a bounded time to land before exit
-    for (int q = 0; q < 1000; ++q) __nanosleep(1000);
+  if (failed && tid == 0 && loads) {
+    // at the break in iteration k: tile planes [kb, min(k + kTile, ke)) were issued and
+    // thread 0 saw [kb, k + 1) land unless one of its waits in this iteration gave up
+    const bool own_fail = lead_fail != 0x7fffffff || tile_fail;
+    mbar_drain(barL, kLead, m_lo, min(lead_fail, mq), m_issued, a.wc.ns);
+    mbar_drain(barT, kTile, kb, own_fail ? k : k + 1, min(k + kTile, ke), a.wc.ns);
   }
 }
 
@@ -752,7 +777,7 @@ struct FilterArgs {
   CUtensorMap mP;           // input buffer, box (TX+8) x (TY+6)
   T* qout;
   const int* runs;          // stored run of each launched run index, or nullptr
-  int* err;
+  WaitCtl wc;               // error word and bound of the ring waits
   Geom g;
   int whole;                // CTAs 0 .. whole-1 filter one (tile, field, face, run) unit each
   int chunks;               // later CTAs filter one of `chunks` radial chunks of a unit
@@ -815,8 +840,11 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) filter_kernel(const _
   // The previous kernel may still be finishing (programmatic launch): the input is read
   // only after the wait.
   grid_dependency_wait();
-  if (tid == 0)
-    for (int k = ks; k < min(ks + kFiltRing, ke); ++k) issue(k, k - ks);
+  // planes [ks, issued) have loads issued; thread 0 has seen planes [ks, seen) land
+  int issued = ks, seen = ks;
+  const bool loads = !a.wc.no_loads;
+  if (tid == 0 && loads)
+    for (; issued < min(ks + kFiltRing, ke); ++issued) issue(issued, issued - ks);
   T* out = a.qout + g.vol(run, face, s) + g.at(0, j0 + ty, i0 + V * cx);
   const T f0 = Coef<T>::filt(0), f1 = Coef<T>::filt(1), f2 = Coef<T>::filt(2), f3 = Coef<T>::filt(3);
   // radial queue of eta-filtered planes; in float the four values of a thread are held as
@@ -841,7 +869,8 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) filter_kernel(const _
     for (int u = 0; u < 11; ++u) {
       const int k = kb + u;
       if (k >= ke) break;
-      ok &= mbar_wait(&bars[slot], phase, a.err, kErrFilterRing);
+      ok = mbar_wait(&bars[slot], phase, a.wc, kErrFilterRing);
+      if (ok) seen = k + 1;
       const T* bx = reinterpret_cast<const T*>(smem + slot * L::P_BYTES);
       T* t1 = reinterpret_cast<T*>(smem + kFiltRing * L::P_BYTES + (k & 1) * L::S_BYTES);
       // xi filter of the box rows (columns V*cx .. V*cx+V-1 of the tile)
@@ -865,7 +894,7 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) filter_kernel(const _
         stv(t1 + r * TX + V * cx, v);
       }
       if (__syncthreads_or(!ok)) { ok = false; break; }
-      if (tid == 0 && k + kFiltRing < ke) issue(k + kFiltRing, slot);
+      if (tid == 0 && loads && k + kFiltRing < ke) { issue(k + kFiltRing, slot); issued = k + kFiltRing + 1; }
       if (++slot == kFiltRing) { slot = 0; phase ^= 1; }
       // eta filter of this thread's V points (rows ty .. ty+6 of the xi-filtered tile)
       T c[7][V];
@@ -922,8 +951,7 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) filter_kernel(const _
     const int k = m < 5 ? m : nr - 10 + m;
     if (k >= ko0 && k < ko1) stv(out + (long long)k * g.plane, zero);
   }
-  if (!ok && tid == 0)
-    for (int q = 0; q < 1000; ++q) __nanosleep(1000);
+  if (!ok && tid == 0) mbar_drain(bars, kFiltRing, ks, seen, issued, a.wc.ns);
 }
 
 // Edge lines exchanged between processes that own different zones: for item q the
@@ -1067,6 +1095,29 @@ __global__ void sumsq_final_kernel(const double* __restrict__ part, int nblocks,
     __syncthreads();
   }
   if (threadIdx.x == 0) out[0] = red[0];
+}
+
+// ---------------------------------------------------------------------------------
+// NaN/Inf watchdog: scans the stored volumes of the owned zones of every run of one buffer
+// (interior, ghost frame and padding -- the frame holds values interpolated from interiors,
+// the padding zeros) with 16-byte loads.  The first launch that sees a non-finite value
+// records its step number in *step_word; later ones leave it.  grid.y = volume
+// ((run * nface + owned face) * nf + slot); grid.x strides over the volume.
+template <typename T>
+__global__ void __launch_bounds__(256) nonfinite_kernel(const T* __restrict__ q, Geom g, int step, int* step_word) {
+  constexpr int V = Vec16<T>::V;
+  const int y = blockIdx.y;
+  const int s = y % g.nf, fz = (y / g.nf) % g.nface, run = y / (g.nf * g.nface);
+  const T* base = q + g.vol(run, g.face0 + fz, s);
+  const long long nv = g.vs / V;
+  bool bad = false;
+  for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += (long long)gridDim.x * blockDim.x) {
+    T x[V];
+    ldv(base + v * V, x);
+#pragma unroll
+    for (int m = 0; m < V; ++m) bad |= !isfinite(x[m]);
+  }
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicCAS(step_word, 0, step);
 }
 
 // ---------------------------------------------------------------------------------

@@ -17,6 +17,10 @@
 
 namespace solar {
 
+static_assert(SOLAR_KERNEL_EDGE == kInjEdge && SOLAR_KERNEL_STAGE == kInjStage && SOLAR_KERNEL_FILTER == kInjFilter &&
+                  SOLAR_KERNEL_ADJ_STAGE == kInjAdjStage,
+              "C-ABI kernel bits and device injection bits agree");
+
 thread_local std::string g_last_error;
 
 static int fail(int code, const char* fmt, ...) {
@@ -106,7 +110,14 @@ struct solar_ctx {
   double* red_out = nullptr;   // reduction result (device)
   int* run_order = nullptr;    // batched runs: stored runs, most steps first
   int run_count = 0;           // runs in the launched grids while a run map is in use
-  int* err = nullptr;          // device error word (bounded waits that gave up)
+  int* err = nullptr;          // device words: [0] error code of a bounded wait that gave up,
+                               // [1] step at which the watchdog first saw a non-finite value
+  int inject_mask = 0;         // failure-injection tests: kernels that issue no loads ...
+  uint32_t inject_ns = 0;      // ... and their wait bound
+  int watch_every = 0;         // NaN/Inf watchdog: check the state every N steps (0 = off)
+  long long steps_done = 0;    // steps taken by this context (watchdog step numbers)
+  double* norm_ring = nullptr; // per-step sums of squares (solar_gpu_rk4_norms)
+  int norm_ring_len = 0;
   DevTables dt;
   int tile_x = 32, tile_y = 8, kchunk = 0, edge_kchunk = 16;
   cudaGraphExec_t step_graph = nullptr;
@@ -185,6 +196,17 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 // Runs covered by a launch: all of them, or the first run_count entries of a run map.
 static int launched_runs(const solar_ctx* c, const int* runs) { return runs ? c->run_count : c->g.nruns; }
 
+// Wait control of one kernel kind (InjectKernel): the error word, the one-second bound,
+// or the failure-injection settings when a test has switched them on for that kernel.
+static WaitCtl wait_ctl(const solar_ctx* c, int kind) {
+  WaitCtl w;
+  w.err = c->err;
+  const bool inj = (c->inject_mask & kind) != 0;
+  w.ns = inj ? c->inject_ns : kWaitNs;
+  w.no_loads = inj ? 1 : 0;
+  return w;
+}
+
 // Launch with programmatic stream serialization: the kernel starts as the previous kernel
 // in the stream retires its last CTAs, does its constant-table prologue, and waits on the
 // device (griddepcontrol.wait) before it touches anything that kernel wrote.  Used for the
@@ -206,8 +228,11 @@ static cudaError_t launch_pdl(void (*kernel)(Args), dim3 grid, dim3 block, size_
 }
 
 // 3-D view of a whole buffer: x = padded column, y = padded row, z = plane index
-// ((run*6 + face)*nf + slot)*nr + k; box bx x by x 1.
-static bool make_map(const solar_ctx* c, const void* base, int bx, int by, CUtensorMap* m) {
+// ((run*6 + face)*nf + slot)*nr + k; box bx x by x 1.  The L2 fetches 256-byte blocks around
+// each request (promotion) unless `promote` is false: boxes whose rows are only a few
+// values wide (the edge kernel's column sources) would otherwise pull whole blocks of
+// unused neighbours from DRAM for every row.
+static bool make_map(const solar_ctx* c, const void* base, int bx, int by, CUtensorMap* m, bool promote = true) {
   auto enc = tensor_map_encoder();
   if (!enc) return false;
   const Geom& g = c->g;
@@ -217,7 +242,8 @@ static bool make_map(const solar_ctx* c, const void* base, int bx, int by, CUten
   cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = enc(m, c->fp32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
                    const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_SWIZZLE_NONE,
+                   promote ? CU_TENSOR_MAP_L2_PROMOTION_L2_256B : CU_TENSOR_MAP_L2_PROMOTION_NONE,
                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
 }
@@ -280,7 +306,7 @@ static int launch_edge(solar_ctx* c, void* buf, int mode, const int* runs) {
     return fail(SOLAR_ERR_ARG, "edge staging window of %d positions is too wide", a.sp);
   if (!make_map(c, buf, a.sp, 3, &a.mRow) || !make_map(c, buf, 4, a.sp, &a.mCol))
     return fail(SOLAR_ERR_CUDA, "cuTensorMapEncodeTiled failed");
-  a.err = c->err;
+  a.wc = wait_ctl(c, kInjEdge);
   static bool attr_set = false;
   if (!attr_set) {
     CK(cudaFuncSetAttribute(edge_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
@@ -357,7 +383,7 @@ static int launch_stage(solar_ctx* c, const void* qin, void* qout, int mode, int
   a.met = (const T*)c->dt.met;
   a.c2 = (const T*)c->dt.c2;
   a.runs = runs;
-  a.err = c->err;
+  a.wc = wait_ctl(c, kInjStage);
   a.g = c->g;
   a.dt = (T)c->desc.dt;
   a.alpha = (T)kAlpha[stage];
@@ -380,7 +406,7 @@ static int launch_filter_t(solar_ctx* c, const void* qin, void* qout, const int*
   if (!make_map(c, qin, TX + 8, TY + 6, &a.mP)) return fail(SOLAR_ERR_CUDA, "cuTensorMapEncodeTiled failed");
   a.qout = (T*)qout;
   a.runs = runs;
-  a.err = c->err;
+  a.wc = wait_ctl(c, kInjFilter);
   a.g = c->g;
   static bool attr_set = false;
   static int resident = 1;
@@ -453,16 +479,48 @@ static int enqueue_step_any(solar_ctx* c, const int* runs, std::vector<cudaEvent
   return c->fp32 ? enqueue_step<float>(c, runs, evs) : enqueue_step<double>(c, runs, evs);
 }
 
-// Device error word: set by a kernel whose bounded wait gave up.
-static int check_device_error(solar_ctx* c) {
-  int h = 0;
-  CK(cudaMemcpyAsync(&h, c->err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
-  if (h) {
-    cudaMemsetAsync(c->err, 0, sizeof(int), c->stream);
-    if (h == kErrForcingSample) return fail(SOLAR_ERR_ARG, "forcing: a time sample outside the loaded samples was needed");
-    return fail(SOLAR_ERR_TIMEOUT, "a device wait gave up (code %d)", h);
+static const char* device_error_name(int code) {
+  switch (code) {
+    case kErrStageLead: return "stage kernel, lead ring";
+    case kErrStageTile: return "stage kernel, tile ring";
+    case kErrFilterRing: return "filter kernel";
+    case kErrEdgeRing: return "edge kernel";
+    case kErrAdjointRing: return "transposed stage kernel";
+    default: return "unknown kernel";
   }
+}
+
+// Device words: [0] set by a kernel whose bounded wait gave up (or by the forcing sampler),
+// [1] the step at which the watchdog first saw a non-finite value.  Both are cleared once
+// read.
+static int check_device_error(solar_ctx* c) {
+  int h[2] = {0, 0};
+  CK(cudaMemcpyAsync(h, c->err, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (h[0] || h[1]) {
+    CK(cudaMemsetAsync(c->err, 0, 2 * sizeof(int), c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  if (h[0] == kErrForcingSample) return fail(SOLAR_ERR_ARG, "forcing: a time sample outside the loaded samples was needed");
+  if (h[0]) return fail(SOLAR_ERR_TIMEOUT, "a device wait gave up (code %d: %s)", h[0], device_error_name(h[0]));
+  if (h[1]) return fail(SOLAR_ERR_NAN, "watchdog: non-finite value in the state after step %d of this context", h[1]);
+  return SOLAR_OK;
+}
+
+// NaN/Inf watchdog: count one step of the context and, every watch_every steps, enqueue a
+// scan of the state buffer (no host wait; check_device_error reports it).
+static int watch_after_step(solar_ctx* c) {
+  ++c->steps_done;
+  if (c->watch_every <= 0 || c->steps_done % c->watch_every) return SOLAR_OK;
+  const Geom& g = c->g;
+  const int V = c->fp32 ? 4 : 2;
+  const long long nv = g.vs / V;
+  const unsigned bx = (unsigned)std::max<long long>(1, std::min<long long>(64, (nv + 2047) / 2048));
+  const dim3 grid(bx, (unsigned)(g.nruns * g.nface * g.nf));
+  const int step = (int)std::min<long long>(c->steps_done, 0x7fffffff);
+  if (c->fp32) nonfinite_kernel<float><<<grid, 256, 0, c->stream>>>((const float*)c->A, g, step, c->err + 1);
+  else nonfinite_kernel<double><<<grid, 256, 0, c->stream>>>((const double*)c->A, g, step, c->err + 1);
+  CK(cudaGetLastError());
   return SOLAR_OK;
 }
 
@@ -641,7 +699,7 @@ int solar_gpu_finalize(solar_ctx* c) {
     if (p) cudaFree(p);
   void* aptrs[] = {c->adj.L, c->adj.LW, c->adj.T1, c->adj.T2, c->adj.rb, c->adj.tspan, c->adj.wt, c->adj.grad, c->adj.ckpt, c->adj.ckpt2,
                    c->adj.div, c->adj.traces, c->adj.rec_off, c->adj.rec_w, c->adj.clk, c->split_items, c->split_slots,
-                   c->force_clock, c->force_exy, c->force_samples, c->force_xy, c->force_r};
+                   c->force_clock, c->force_exy, c->force_samples, c->force_xy, c->force_r, c->norm_ring};
   for (void* p : aptrs)
     if (p) cudaFree(p);
   for (auto& e : c->ev)
@@ -735,8 +793,8 @@ int solar_gpu_init(const solar_desc* d, solar_ctx** out) {
   TRYC(cudaMalloc((void**)&c->dt.s0t, c->ht.s0t.size() * sizeof(int)));
   TRYC(cudaMemcpy(c->dt.s0t, c->ht.s0t.data(), c->ht.s0t.size() * sizeof(int), cudaMemcpyHostToDevice));
   TRY(edge_windows(c));
-  TRYC(cudaMalloc((void**)&c->err, sizeof(int)));
-  TRYC(cudaMemset(c->err, 0, sizeof(int)));
+  TRYC(cudaMalloc((void**)&c->err, 2 * sizeof(int)));
+  TRYC(cudaMemset(c->err, 0, 2 * sizeof(int)));
   if (!tensor_map_encoder()) { solar_gpu_finalize(c); return fail(SOLAR_ERR_CUDA, "cuTensorMapEncodeTiled entry point unavailable"); }
   TRY(upload<double>((void**)&c->dt.rad64, c->ht.radial));
   {
@@ -805,7 +863,10 @@ int solar_gpu_rk4(solar_ctx* c, int nsteps) {
   if (rc) return rc;
   if (nsteps < 0) return fail(SOLAR_ERR_ARG, "nsteps < 0");
   if ((rc = capture_step_graph(c))) return rc;
-  for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(c->step_graph, c->stream));
+  for (int s = 0; s < nsteps; ++s) {
+    CK(cudaGraphLaunch(c->step_graph, c->stream));
+    if ((rc = watch_after_step(c))) return rc;
+  }
   CK(cudaStreamSynchronize(c->stream));
   return check_device_error(c);
 }
@@ -845,7 +906,10 @@ static int rk4_runs_impl(solar_ctx* c, const int* nsteps_per_run, double* ms) {
     if ((rc = capture_batch_graph(c, st.first))) return rc;
   CK(cudaEventRecord(c->ev[0], c->stream));
   for (const auto& st : stretches)
-    for (int s = 0; s < st.second; ++s) CK(cudaGraphLaunch(c->batch_graphs[st.first], c->stream));
+    for (int s = 0; s < st.second; ++s) {
+      CK(cudaGraphLaunch(c->batch_graphs[st.first], c->stream));
+      if ((rc = watch_after_step(c))) return rc;
+    }
   CK(cudaEventRecord(c->ev[1], c->stream));
   CK(cudaStreamSynchronize(c->stream));
   if (ms) {
@@ -978,7 +1042,10 @@ int solar_gpu_time_rk4(solar_ctx* c, int nsteps, int per_kernel, double* out7) {
   if (!per_kernel) {
     if ((rc = capture_step_graph(c))) return rc;
     CK(cudaEventRecord(c->ev[0], c->stream));
-    for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(c->step_graph, c->stream));
+    for (int s = 0; s < nsteps; ++s) {
+      CK(cudaGraphLaunch(c->step_graph, c->stream));
+      if ((rc = watch_after_step(c))) return rc;
+    }
     CK(cudaEventRecord(c->ev[1], c->stream));
     CK(cudaEventSynchronize(c->ev[1]));
     float ms = 0;
@@ -988,8 +1055,10 @@ int solar_gpu_time_rk4(solar_ctx* c, int nsteps, int per_kernel, double* out7) {
   }
   std::vector<cudaEvent_t> evs;
   CK(cudaEventRecord(c->ev[0], c->stream));
-  for (int s = 0; s < nsteps; ++s)
+  for (int s = 0; s < nsteps; ++s) {
     if ((rc = enqueue_step_any(c, nullptr, &evs))) return rc;
+    if ((rc = watch_after_step(c))) return rc;
+  }
   CK(cudaEventRecord(c->ev[1], c->stream));
   CK(cudaEventSynchronize(c->ev[1]));
   float ms = 0;
@@ -1021,6 +1090,65 @@ int solar_gpu_time_rk4(solar_ctx* c, int nsteps, int per_kernel, double* out7) {
   if (out7[5] > 0) out7[2] /= out7[5];
   if (out7[6] > 0) out7[3] /= out7[6];
   return check_device_error(c);
+}
+
+int solar_gpu_rk4_norms(solar_ctx* c, int run, int field, int nsteps, double* norms) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!norms || nsteps < 0 || field < 1 || field > 5 || run < 0 || run >= c->g.nruns)
+    return fail(SOLAR_ERR_ARG, "bad run, field, step count or null output");
+  if (nsteps == 0) return SOLAR_OK;
+  if (c->norm_ring_len < nsteps) {
+    CK(cudaStreamSynchronize(c->stream));
+    if (c->norm_ring) cudaFree(c->norm_ring);
+    c->norm_ring = nullptr;
+    c->norm_ring_len = 0;
+    cudaError_t e = cudaMalloc((void**)&c->norm_ring, (size_t)nsteps * sizeof(double));
+    if (e != cudaSuccess) return fail(SOLAR_ERR_NOMEM, "per-step norms: %s", cudaGetErrorString(e));
+    c->norm_ring_len = nsteps;
+  }
+  if ((rc = capture_step_graph(c))) return rc;
+  const int slot = c->g.slot[field - 1];
+  const int nblocks = c->g.nface * c->g.nr;
+  if (slot < 0) CK(cudaMemsetAsync(c->norm_ring, 0, (size_t)nsteps * sizeof(double), c->stream));
+  for (int s = 0; s < nsteps; ++s) {
+    CK(cudaGraphLaunch(c->step_graph, c->stream));
+    if ((rc = watch_after_step(c))) return rc;
+    if (slot < 0) continue;
+    if (c->fp32) sumsq_plane_kernel<float><<<nblocks, 256, 0, c->stream>>>((const float*)c->A, c->g, run, slot, c->part);
+    else sumsq_plane_kernel<double><<<nblocks, 256, 0, c->stream>>>((const double*)c->A, c->g, run, slot, c->part);
+    sumsq_final_kernel<<<1, 256, 0, c->stream>>>(c->part, nblocks, c->norm_ring + s);
+    CK(cudaGetLastError());
+  }
+  CK(cudaMemcpyAsync(norms, c->norm_ring, (size_t)nsteps * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  // auxiliary.f90:122, as solar_gpu_norm
+  const double npts = (double)c->g.n * c->g.n * c->g.nr;
+  for (int s = 0; s < nsteps; ++s) norms[s] = std::pow(norms[s] / npts * 6.0, 0.5);
+  return check_device_error(c);
+}
+
+int solar_gpu_set_watchdog(solar_ctx* c, int every) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (every < 0) return fail(SOLAR_ERR_ARG, "watchdog interval must be >= 0");
+  c->watch_every = every;
+  return SOLAR_OK;
+}
+
+int solar_gpu_inject_wait_timeout(solar_ctx* c, int kernels, int wait_us) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (kernels & ~(SOLAR_KERNEL_EDGE | SOLAR_KERNEL_STAGE | SOLAR_KERNEL_FILTER | SOLAR_KERNEL_ADJ_STAGE))
+    return fail(SOLAR_ERR_ARG, "unknown kernel bits 0x%x", kernels);
+  if (kernels && (wait_us < 1 || wait_us > 1000000)) return fail(SOLAR_ERR_ARG, "wait_us must be in 1..1000000");
+  CK(cudaStreamSynchronize(c->stream));
+  c->inject_mask = kernels;
+  c->inject_ns = kernels ? (uint32_t)wait_us * 1000u : 0u;
+  // the captured step graphs hold the old launch arguments
+  if (c->step_graph) { cudaGraphExecDestroy(c->step_graph); c->step_graph = nullptr; }
+  drop_batch_graphs(c);
+  return SOLAR_OK;
 }
 
 int solar_gpu_synchronize(solar_ctx* c) {

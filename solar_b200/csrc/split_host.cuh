@@ -106,7 +106,7 @@ int solar_gpu_step_phase(solar_ctx* c, int phase) {
   rc = c->fp32 ? enqueue_phase<float>(c, phase) : enqueue_phase<double>(c, phase);
   if (rc) return rc;
   CK(cudaGetLastError());
-  return SOLAR_OK;
+  return phase == 5 ? watch_after_step(c) : SOLAR_OK;
 }
 
 long long solar_gpu_lines_size(solar_ctx* c, int phase) {

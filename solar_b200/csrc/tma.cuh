@@ -2,8 +2,15 @@
 // and shared-memory mbarriers used by the streaming stencil kernels.
 //
 // Only plain (single-CTA) tile loads are used: every load reads this GPU's own memory.
-// Every wait on an mbarrier is bounded: after kWaitLimit polls the caller gets `false`,
-// records an error flag for the host and leaves its loop.
+//
+// Every wait on an mbarrier is bounded by time (the global nanosecond timer): after the
+// kernel's limit (kWaitNs, one second) the waiting thread gets `false` and records an
+// error code in the context's device error word, which the host turns into
+// SOLAR_ERR_TIMEOUT.  A CTA whose wait gave up stops issuing loads, leaves its plane loop
+// at the next CTA barrier and, before it exits, waits (bounded again) for every load it
+// issued and did not consume, so that no bulk copy is still writing into its shared
+// memory when the SM hands that memory to another CTA.  A copy that has not landed after
+// a second limit is taken as lost.
 #pragma once
 
 #include <cuda.h>
@@ -12,7 +19,7 @@
 
 namespace solar {
 
-constexpr uint32_t kWaitLimit = 1u << 22;   // polls of try_wait before giving up
+constexpr uint32_t kWaitNs = 1000000000u;   // bound of one wait: 1 s
 
 // Codes a kernel leaves in the context's device error word.
 enum DeviceError : int {
@@ -22,6 +29,18 @@ enum DeviceError : int {
   kErrEdgeRing = 4,         // edge kernel: ring wait gave up
   kErrAdjointRing = 5,      // transposed stage kernel: ring wait gave up
   kErrForcingSample = 16,   // a forcing time sample outside the loaded samples was needed
+};
+
+// Kernels that take part in failure-injection tests (solar_gpu_inject_wait_timeout).
+enum InjectKernel : int { kInjEdge = 1, kInjStage = 2, kInjFilter = 4, kInjAdjStage = 8 };
+
+// Wait control carried in a kernel's arguments: the device error word, the bound of one
+// wait in nanoseconds, and the injection switch of failure-detection tests (nonzero: the
+// producer issues no loads, so the first wait runs out with nothing in flight).
+struct WaitCtl {
+  int* err;
+  uint32_t ns;
+  int no_loads;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -52,12 +71,39 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait for the phase with the given parity to complete.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code) {
-  for (uint32_t it = 0; it < kWaitLimit; ++it)
-    if (mbar_try_wait(bar, parity)) return true;
-  if (err) atomicExch(err, code);
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Wait at most limit_ns for the phase with the given parity to complete.
+__device__ __forceinline__ bool mbar_wait_ns(uint64_t* bar, uint32_t parity, uint32_t limit_ns) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (;;) {
+#pragma unroll 1
+    for (int i = 0; i < 32; ++i)
+      if (mbar_try_wait(bar, parity)) return true;
+    if (global_ns() - t0 > limit_ns) return false;
+  }
+}
+
+// Consumer wait: on giving up, record `code` in the device error word.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, const WaitCtl& w, int code) {
+  if (mbar_wait_ns(bar, parity, w.ns)) return true;
+  if (w.err) atomicExch(w.err, code);
   return false;
+}
+
+// Before a CTA that gave up exits: wait (bounded) for the loads of planes [first, end) of a
+// ring of `slots` mbarriers filled in plane order from plane `base` (plane m in slot
+// (m - base) % slots, phase parity ((m - base) / slots) & 1).
+__device__ __forceinline__ void mbar_drain(uint64_t* bars, int slots, int base, int first, int end, uint32_t limit_ns) {
+  for (int m = first; m < end; ++m) {
+    const int q = m - base;
+    mbar_wait_ns(&bars[q % slots], (uint32_t)((q / slots) & 1), limit_ns);
+  }
 }
 
 // 3-D tile load global -> shared, completion signalled on `bar` (transaction bytes).

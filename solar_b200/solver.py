@@ -130,6 +130,18 @@ class Solver:
         """``nsteps`` calls of the reference's RK4 (timestep.f90:41-86) on every run."""
         _lib.check(self.lib.solar_gpu_rk4(self._h, int(nsteps)))
 
+    def rk4_norms(self, nsteps: int, field: int = 4, run: int = 0, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """The loop of cube.f90:71-79: ``nsteps`` RK4 calls, each followed by the norm of
+        ``field`` (auxiliary.f90:100-125); the norms are read back once, after the last step."""
+        norms = np.empty(int(nsteps)) if out is None else out
+        _lib.check(self.lib.solar_gpu_rk4_norms(self._h, int(run), int(field), int(nsteps), _ptr(norms)))
+        return norms
+
+    def set_watchdog(self, every: int) -> None:
+        """Scan the state for NaN/Inf every ``every`` steps (0 = off); a hit makes the
+        stepping call raise SolarError with status SOLAR_ERR_NAN."""
+        _lib.check(self.lib.solar_gpu_set_watchdog(self._h, int(every)))
+
     def rk4_runs(self, steps: Sequence[int]) -> None:
         """Advance run r by steps[r] RK4 steps (uneven counts, one batched graph)."""
         s = np.ascontiguousarray(np.asarray(steps, dtype=np.int32))
