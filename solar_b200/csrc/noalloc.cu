@@ -13,13 +13,24 @@
 // plane) -- in a fixed-size file-scope device array.
 //
 // Limits and sharing.  The array holds kNormMaxPlanes partials, so nr <= kNormMaxPlanes/6
-// (2048); larger grids are rejected with SOLAR_ERR_ARG.  Every GPU that loads the library
+// (2048); larger grids, and planes of more than INT_MAX points, are rejected with
+// SOLAR_ERR_ARG before anything is launched.  Every GPU that loads the library
 // holds the array (96 KiB) until the process exits.  All calls share it and it keeps the
 // previous call's partials; each call overwrites exactly the partials it then reads, so
 // nothing has to be cleared first.  Two calls whose kernels overlap on the GPU (different
 // streams, same device) race on the array: serialise them.
+//
+// Set-up.  The array's device address is resolved with cudaGetSymbolAddress (which
+// allocates nothing) on the first call in each CUDA context, with that context current,
+// and cached together with the context's unique id: after a cudaDeviceReset the device
+// gets a new primary context, the module is loaded again, and the next call resolves the
+// new address instead of using a dead one.  That first call per context should come
+// before any stream capture.
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
+#include <climits>
 #include <cstdio>
 #include <mutex>
 
@@ -37,9 +48,36 @@ constexpr int kThreads = 256;
 
 static __device__ __align__(256) double g_norm_partials[kNormMaxPlanes];
 
-// Device address of g_norm_partials, per device (nullptr until that device is set up).
+// Device address of g_norm_partials per device, valid for the context whose id is cached
+// beside it (nullptr until that device is set up).
 double* g_partials[kMaxDevices] = {};
+unsigned long long g_ctx_id[kMaxDevices] = {};
 std::mutex g_setup_mutex;
+
+// Unique id of the calling thread's current CUDA context (driver entry points reached
+// through the runtime, so the library needs no -lcuda); 0 when unavailable.
+unsigned long long current_context_id() {
+  static PFN_cuCtxGetCurrent_v4000 get_current = nullptr;
+  static PFN_cuCtxGetId_v12000 get_id = nullptr;
+  static bool looked_up = false;
+  if (!looked_up) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(p);
+    p = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<PFN_cuCtxGetId_v12000>(p);
+    looked_up = true;
+  }
+  if (!get_current || !get_id) return 0;
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
 
 // One CTA per (zone, plane): sum of f^2 over the plane in a fixed order.
 __global__ void __launch_bounds__(kThreads) norm_plane_sums(const double* __restrict__ f, int plane,
@@ -77,6 +115,8 @@ __global__ void __launch_bounds__(kThreads) norm_finish(const double* __restrict
 extern "C" int solar_gpu_norm_noalloc(const double* d_field, int nx, int nr, double* d_out, void* stream) {
   if (!d_field || !d_out) return solar::report_error(SOLAR_ERR_ARG, "solar_gpu_norm_noalloc: null device pointer");
   if (nx < 1 || nr < 1) return solar::report_error(SOLAR_ERR_ARG, "solar_gpu_norm_noalloc: nx and nr must be >= 1");
+  if ((long long)nx * nx > INT_MAX)
+    return solar::report_error(SOLAR_ERR_ARG, "solar_gpu_norm_noalloc: nx * nx exceeds INT_MAX points per plane");
   if (6LL * nr > kNormMaxPlanes) {
     char msg[160];
     std::snprintf(msg, sizeof(msg),
@@ -90,16 +130,23 @@ extern "C" int solar_gpu_norm_noalloc(const double* d_field, int nx, int nr, dou
   if (dev < 0 || dev >= kMaxDevices) return solar::report_error(SOLAR_ERR_ARG, "solar_gpu_norm_noalloc: device ordinal too large");
   double* part = nullptr;
   {
-    // First call on a device (that device current): resolve the array's device address.
+    // First call in a context (that context current): resolve the array's device address.
     // The host-side name g_norm_partials is only a stand-in; kernels need this address.
+    // (cudaGetSymbolAddress also creates the device's primary context if it does not exist
+    // yet, so the id is read after it.)  Without a context id the address is resolved on
+    // every call.
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_partials[dev]) {
+    const unsigned long long id = current_context_id();
+    if (g_partials[dev] && id != 0 && g_ctx_id[dev] == id) {
+      part = g_partials[dev];
+    } else {
       void* p = nullptr;
       e = cudaGetSymbolAddress(&p, g_norm_partials);
       if (e != cudaSuccess) return solar::report_error(SOLAR_ERR_CUDA, cudaGetErrorString(e));
-      g_partials[dev] = static_cast<double*>(p);
+      part = static_cast<double*>(p);
+      g_partials[dev] = part;
+      g_ctx_id[dev] = current_context_id();
     }
-    part = g_partials[dev];
   }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int planes = 6 * nr;

@@ -79,3 +79,22 @@ def test_null_context_is_an_error_not_a_crash(lib):
     assert lib.solar_gpu_rk4(None, 1) == -5
     assert lib.solar_gpu_get_state(None, 0, q.ctypes.data_as(ctypes.POINTER(ctypes.c_double))) == -5
     assert lib.solar_gpu_finalize(None) == 0
+
+
+def test_new_entry_points_reject_a_null_context(lib):
+    out = np.zeros(4)
+    p = out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    assert lib.solar_gpu_rk4_norms(None, 0, 4, 2, p) == -5
+    assert lib.solar_gpu_set_watchdog(None, 1) == -5
+    assert lib.solar_gpu_inject_wait_timeout(None, 1, 100) == -5
+
+
+def test_norm_noalloc_rejects_planes_beyond_int_range_before_any_launch(lib):
+    # nx * nx > INT_MAX would overflow the kernel's plane size: refused on the host, before
+    # the device is touched (the pointers are never dereferenced).
+    fake = ctypes.c_void_p(4096)
+    assert lib.solar_gpu_norm_noalloc(fake, 46341, 4, fake, None) == -1
+    assert "INT_MAX" in _lib.last_error()
+    assert lib.solar_gpu_norm_noalloc(fake, 16, 4096, fake, None) == -1
+    assert "exceeds" in _lib.last_error()
+    assert lib.solar_gpu_norm_noalloc(None, 16, 16, fake, None) == -1
