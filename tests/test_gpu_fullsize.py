@@ -1,5 +1,11 @@
-"""Parity at the workloads' full sizes, through properties that do not need the oracle (which
-is too slow at these sizes):
+"""Parity at the workloads' full sizes.
+
+Against the oracle at the benchmark's 6 x 128^3 (ten full RK4 steps from a state with
+Gaussian blobs on every cube corner and edge, so every inter-zone edge and both radial
+ends take part): the FP64 path <= 1e-11 relative L2 per field, the FP32 path <= 1e-5 per
+field; the per-field maximum errors are printed (run with -s).
+
+Through properties that do not need the oracle (too slow for more steps at these sizes):
 
 * linearity of the FP64 step at 6 x 128^3: STEP(a q1 + b q2) = a STEP(q1) + b STEP(q2), to
   rounding (1e-12 relative);
@@ -9,6 +15,9 @@ is too slow at these sizes):
 * batched uneven runs at 64 x 6 x 64^3 equal the same runs stepped alone, bit for bit;
 * the zones split over 3 emulated processes at 6 x 128^3 equal the one-context run, bit for bit.
 """
+import json
+import os
+
 import numpy as np
 import pytest
 
@@ -40,6 +49,52 @@ def blobs(cfg, seed, n=4):
 @pytest.fixture(scope="module")
 def c2():
     return configs.c2()
+
+
+def edge_and_corner_blobs(o, cfg):
+    """Five fields of Gaussian blobs (width 0.08): v_xi and v_eta on the 8 cube corners,
+    rho, v_r and p on the 12 cube-edge midpoints, at seeded radii inside the shell."""
+    rng = np.random.default_rng(12)
+    corners = np.array([(x, y, z) for x in (-1, 1) for y in (-1, 1) for z in (-1, 1)], float)
+    mids = np.array([v for i in range(3) for a in (-1, 1) for b in (-1, 1)
+                     for v in [np.insert(np.array([a, b], float), i, 0.0)]])
+    r0, r1 = float(cfg.model[0, 0]), float(cfg.model[-1, 0])
+    q = np.zeros(o.state_shape)
+    for f, dirs in ((0, mids), (1, corners), (2, corners), (3, mids), (4, mids)):
+        srcs = []
+        for d in dirs:
+            d = d / np.linalg.norm(d) * rng.uniform(r0 + 0.25 * (r1 - r0), r0 + 0.8 * (r1 - r0))
+            srcs.append(configs.Source(tuple(d), 0.08, rng.uniform(0.5, 1.5)))
+        q[:, f] = o.initial_state(srcs)[:, 4]
+    return q
+
+
+ORACLE_STEPS = 10
+
+
+def test_fp64_and_fp32_match_the_oracle_at_c2(c2, oracle_mod):
+    oracle_mod.set_threads(os.cpu_count() or 1)
+    o = oracle_mod.Oracle(c2)
+    q0 = edge_and_corner_blobs(o, c2)
+    ref = o.rk4(q0, ORACLE_STEPS)
+    got = {}
+    for prec, nf in (("fp64", 5), ("fp32", 4)):
+        with Solver(c2, precision=prec, nfields=nf) as s:
+            s.set_state(q0)
+            s.rk4(ORACLE_STEPS)
+            got[prec] = s.get_state()
+    names = ("rho", "v_xi", "v_eta", "v_r", "p")
+    report = {}
+    for prec, fields in (("fp64", range(5)), ("fp32", range(1, 5))):
+        for f in fields:
+            d = got[prec][:, f] - ref[:, f]
+            report[f"{prec}.{names[f]}"] = {"rel_l2": rel(got[prec][:, f], ref[:, f]),
+                                           "max_abs_over_max_ref": float(np.abs(d).max() / np.abs(ref[:, f]).max())}
+    print("c2 6x128^3, %d steps vs the oracle: %s" % (ORACLE_STEPS, json.dumps(report)))
+    for f in range(5):
+        assert report[f"fp64.{names[f]}"]["rel_l2"] <= 1e-11, (names[f], report)
+    for f in range(1, 5):
+        assert report[f"fp32.{names[f]}"]["rel_l2"] <= 1e-5, (names[f], report)
 
 
 def test_step_is_linear_at_c2(c2):
