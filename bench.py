@@ -11,8 +11,11 @@ grid point advanced one full step.
 * fp64        the plain FP64 path (5 fields) on the same workload, for the FP32-vs-FP64
               comparison; fp32_rel_err_vs_fp64 is the per-field relative L2 after the run.
 * e2e         the same metric through the C-ABI with host buffers: state uploaded from
-              pinned host memory, RK4 called once per step with the reference's per-step
-              norm (cube.f90:77) read back, final state downloaded.
+              pinned host memory, K steps of RK4 each followed by the reference's per-step
+              norm (cube.f90:77; solar_gpu_rk4_norms, read back once after the last step),
+              final state downloaded.  fp64.e2e is the same for the FP64 path.
+* fp32_err_c2_1000  FP32 (4 fields) against FP64 (5 fields) after 1000 steps of the
+              workload: per-field relative L2 and max |difference| / max |FP64|.
 * roofline    the dominant kernel (the fused stage kernel): algorithmic bytes per launch
               (q and qw read, q and qw written; 3F words in stage 1, 4F in stages 2-5)
               over its mean launch time from per-launch CUDA events.
@@ -212,9 +215,10 @@ def rel_errors(a, b, fields):
 
 def adjoint_block(device: int, nsteps: int, k: int, nfd: int):
     """Misfit gradient dJ/dc on the adjoint workload (6 x 96^3 stratified shell, 32 receivers
-    at r = 0.98, data from a model with eight sound-speed anomalies), timed on the device,
-    and checked against central finite differences of the GPU FP64 misfit along nfd
-    directions (half random per point, half smooth blobs near the anomalies)."""
+    at r = 0.98, data from a model with eight sound-speed anomalies), timed on the device in
+    FP32 (4 fields) and FP64 (5 fields).  The FP32 gradient is checked against the FP64 one
+    (relative L2), and both against central finite differences of the GPU FP64 misfit along
+    nfd directions (half random per point, half smooth blobs near the anomalies)."""
     import numpy as np
     from solar_b200 import configs, receivers
     from solar_b200.solver import Solver
@@ -233,16 +237,19 @@ def adjoint_block(device: int, nsteps: int, k: int, nfd: int):
             s.set_receivers(loc)
             return s.record(nsteps)
 
+    def gradient(prec, nf):
+        with Solver(cfg, precision=prec, nfields=nf, device=device, c2_3d=c0 ** 2) as s:
+            s.set_state(q0)
+            s.set_receivers(loc)
+            s.misfit_gradient(min(k, nsteps), k, data[:min(k, nsteps)])      # warm-up, allocates
+            return s.misfit_gradient(nsteps, k, data)
+
     data = traces(c_true)
-    with Solver(cfg, device=device, c2_3d=c0 ** 2) as s:
-        s.set_state(q0)
-        s.set_receivers(loc)
-        s.misfit_gradient(min(k, nsteps), k, data[:min(k, nsteps)])      # warm-up, allocates
-        res = s.misfit_gradient(nsteps, k, data)
-    grad = res["grad_c"]
-    total_ms = res["forward_ms"] + res["recompute_ms"] + res["adjoint_ms"]
+    res64 = gradient("fp64", 5)
+    res32 = gradient("fp32", 4)
+    g64, g32 = res64["grad_c"], res32["grad_c"]
     rng = np.random.default_rng(44)
-    errs = []
+    errs64, errs32 = [], []
     for m in range(nfd):
         if m % 2 == 0:
             d = rng.standard_normal(c0.shape) * c0
@@ -256,19 +263,87 @@ def adjoint_block(device: int, nsteps: int, k: int, nfd: int):
         jp = 0.5 * float(((traces(c0 + eps * d) - data) ** 2).sum())
         jm = 0.5 * float(((traces(c0 - eps * d) - data) ** 2).sum())
         fd = (jp - jm) / (2 * eps)
-        ad = float(np.vdot(grad.ravel(), d.ravel()))
-        errs.append(abs(fd - ad) / abs(ad))
+        for g, errs in ((g64, errs64), (g32, errs32)):
+            ad = float(np.vdot(g.ravel(), d.ravel()))
+            errs.append(abs(fd - ad) / abs(fd))
     pts = cfg.points
-    return {
-        "workload": "c4: 6 x %d^3 stratified shell, %d steps, %d receivers, checkpoint every %d steps, FP64" % (
-            cfg.nx, nsteps, len(loc), k),
-        "misfit": res["misfit"], "gradient_ms": total_ms,
-        "forward_ms": res["forward_ms"], "recompute_ms": res["recompute_ms"], "adjoint_ms": res["adjoint_ms"],
-        "adjoint_pt_steps_per_s": pts * nsteps / (res["adjoint_ms"] / 1e3),
-        "gradient_cost_in_forward_runs": total_ms / res["forward_ms"],
-        "fd_directions": nfd, "fd_rel_err_max": max(errs) if errs else None,
-        "fd_rel_errs": errs, "fd_tolerance": 1e-4,
-    }
+
+    def timing(res):
+        total_ms = res["forward_ms"] + res["recompute_ms"] + res["adjoint_ms"]
+        return {"misfit": res["misfit"], "gradient_ms": total_ms, "forward_ms": res["forward_ms"],
+                "recompute_ms": res["recompute_ms"], "adjoint_ms": res["adjoint_ms"],
+                "adjoint_pt_steps_per_s": pts * nsteps / (res["adjoint_ms"] / 1e3),
+                "gradient_cost_in_forward_runs": total_ms / res["forward_ms"]}
+
+    out = {"workload": "c4: 6 x %d^3 stratified shell, %d steps, %d receivers, checkpoint every %d steps" % (
+        cfg.nx, nsteps, len(loc), k)}
+    out["fp32"] = timing(res32)
+    out["fp32"]["fields"] = 4
+    out["fp32"]["grad_rel_l2_vs_fp64"] = float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64))
+    out["fp32"]["fd_rel_err_max"] = max(errs32) if errs32 else None
+    out["fp32"]["fd_rel_errs"] = errs32
+    out["fp64"] = timing(res64)
+    out["fp64"]["fields"] = 5
+    out["fp64"]["fd_rel_err_max"] = max(errs64) if errs64 else None
+    out["fp64"]["fd_rel_errs"] = errs64
+    out["fd_directions"] = nfd
+    out["fd_reference"] = "central differences of the GPU FP64 misfit, eps = 1e-6 relative"
+    out["fd_tolerance"] = 1e-4
+    return out
+
+
+def fp32_error_block(cfg, device: int, nsteps: int):
+    """FP32 (4 fields) against FP64 (5 fields) on the benchmark workload after nsteps steps:
+    per-field relative L2 and max |FP32 - FP64| / max |FP64|."""
+    from solar_b200.solver import Solver
+
+    states = {}
+    for prec, nf in (("fp64", 5), ("fp32", 4)):
+        with Solver(cfg, precision=prec, nfields=nf, device=device) as s:
+            s.init_sources()
+            s.rk4(nsteps)
+            states[prec] = s.get_state()
+    a, b = states["fp32"], states["fp64"]
+    names = ("rho", "v_xi", "v_eta", "v_r", "p")
+    out = {"steps": nsteps}
+    for m in (1, 2, 3, 4):
+        out[names[m]] = {"rel_l2": float(np.linalg.norm(a[:, m] - b[:, m]) / np.linalg.norm(b[:, m])),
+                         "max_abs_over_max_ref": float(np.abs(a[:, m] - b[:, m]).max() / np.abs(b[:, m]).max())}
+    out["max_rel_l2"] = max(out[names[m]]["rel_l2"] for m in (1, 2, 3, 4))
+    out["tolerance"] = 1e-5
+    return out
+
+
+def e2e_block(cfg, precision: str, nfields: int, args, world: int, local: int):
+    """End to end through the C-ABI with host buffers: the six-zone FP64 state comes in from
+    pinned host memory, K steps run with the per-step norm of v_r (cube.f90:74-78), the
+    norms and the final state come back to pinned host memory.  Host wall clock around the
+    whole job; max over ranks."""
+    import torch
+    from solar_b200.solver import Solver
+
+    state_bytes = 6 * 5 * cfg.nr * cfg.nx * cfg.nx * 8
+    host = torch.empty(6 * 5 * cfg.nr * cfg.nx * cfg.nx, dtype=torch.float64, pin_memory=True).numpy()
+    out = torch.empty_like(torch.from_numpy(host)).pin_memory().numpy()
+    norms = torch.empty(args.steps, dtype=torch.float64, pin_memory=True).numpy()
+    with Solver(cfg, precision=precision, nfields=nfields, device=local) as se:
+        se.init_sources()
+        se.get_state(out=host.reshape(se.state_shape))
+        se.rk4_norms(args.warmup, out=norms[:args.warmup] if args.warmup <= args.steps else None)
+        barrier(world)
+        t0 = time.perf_counter()
+        se.set_state(host.reshape(se.state_shape))
+        se.rk4_norms(args.steps, out=norms)
+        se.get_state(out=out.reshape(se.state_shape))
+        te = time.perf_counter() - t0
+    te = max_over_ranks(te, world)
+    return {"value": cfg.points * args.steps * world / te, "unit": "grid-pt RK4 updates/s",
+            "h2d_bytes_per_step": state_bytes / args.steps,
+            "d2h_bytes_per_step": (state_bytes + 8 * args.steps) / args.steps,
+            "ms_per_step": te * 1e3 / args.steps, "norm_vr_last": float(norms[-1]),
+            "note": "state in from pinned host memory once per job, K RK4 steps each followed by "
+                    "norm(v_r) (cube.f90:74-78) kept on the device and read back once, state out at "
+                    "the end; host wall clock of the whole job"}
 
 
 def batch_block(device: int):
@@ -308,12 +383,16 @@ def large_block(device: int, nsteps: int):
     cfg = configs.c5(nsteps=nsteps)
     out = {"workload": "c5: 6 x %d^3, %d steps" % (cfg.nx, nsteps)}
     for prec, nf in (("fp32", 4), ("fp64", 5)):
-        with Solver(cfg, precision=prec, nfields=nf, device=device) as s:
+        t0 = time.perf_counter()
+        s = Solver(cfg, precision=prec, nfields=nf, device=device)
+        init_s = time.perf_counter() - t0
+        with s:
             s.init_sources()
             s.rk4(3)
             t = s.time_rk4(nsteps)
             out[prec] = {"value": cfg.points * nsteps / (t["total_ms"] / 1e3), "ms_per_step": t["total_ms"] / nsteps,
-                         "fields": nf, "norm_vr": s.norm(4)}
+                         "fields": nf, "norm_vr": s.norm(4),
+                         "init_s": init_s}    # solar_gpu_init: host tables, uploads, state buffers
     out["fp32_speedup"] = out["fp32"]["value"] / out["fp64"]["value"]
     return out
 
@@ -396,14 +475,18 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--adjoint-steps", type=int, default=500)
     ap.add_argument("--adjoint-checkpoint", type=int, default=50)
-    ap.add_argument("--adjoint-fd", type=int, default=4)
+    ap.add_argument("--adjoint-fd", type=int, default=16)
+    ap.add_argument("--err-steps", type=int, default=1000,
+                    help="steps of the FP32-vs-FP64 error check on the workload (0 = skip)")
     ap.add_argument("--split", action="store_true",
                     help="also run the zones split across the job's processes (world must divide 6)")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-large", action="store_true")
     ap.add_argument("--large-steps", type=int, default=200)
-    ap.add_argument("--large-adjoint", action="store_true",
-                    help="also run the misfit gradient on the 6 x 384^3 grid (about 160 GB of device memory)")
+    ap.add_argument("--no-large-adjoint", action="store_true",
+                    help="skip the misfit gradient on the 6 x 384^3 grid")
+    ap.add_argument("--large-adjoint-steps", type=int, default=20,
+                    help="steps of the 6 x 384^3 misfit gradient (200 = the workload's full run, ~160 GB)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -458,31 +541,10 @@ def main():
     err = rel_errors(q32, q64, (1, 2, 3, 4))
 
     # ---------------------------------------------------------------- end to end (C-ABI, host buffers)
-    e2e = None
+    e2e = e2e64 = None
     if not args.no_e2e:
-        import torch
-        state_bytes = 6 * 5 * cfg.nr * cfg.nx * cfg.nx * 8
-        host = torch.empty(6 * 5 * cfg.nr * cfg.nx * cfg.nx, dtype=torch.float64, pin_memory=True).numpy()
-        out = torch.empty_like(torch.from_numpy(host)).pin_memory().numpy()
-        with Solver(cfg, precision="fp32", nfields=4, device=local) as se:
-            se.init_sources()
-            se.get_state(out=host.reshape(se.state_shape))
-            se.rk4(args.warmup)
-            barrier(world)
-            t0 = time.perf_counter()
-            se.set_state(host.reshape(se.state_shape))
-            norms = []
-            for _ in range(args.steps):
-                se.rk4(1)
-                norms.append(se.norm(4))
-            se.get_state(out=out.reshape(se.state_shape))
-            te = time.perf_counter() - t0
-        te = max_over_ranks(te, world)
-        e2e = {"value": pts * args.steps * world / te, "unit": "grid-pt RK4 updates/s",
-               "h2d_bytes_per_step": state_bytes / args.steps,
-               "d2h_bytes_per_step": state_bytes / args.steps + 8,
-               "note": "state in from pinned host memory once, RK4 + norm(v_r) read back every step "
-                       "(cube.f90:74-78), state out at the end; timed per job of K steps"}
+        e2e = e2e_block(cfg, "fp32", 4, args, world, local)
+        e2e64 = e2e_block(cfg, "fp64", 5, args, world, local)
 
     split = split_block(cfg, args, world, local) if args.split else None
     if rank != 0:
@@ -495,8 +557,11 @@ def main():
     if world == 1 and not args.no_large:
         large = large_block(local, args.large_steps)
     large_adj = None
-    if world == 1 and args.large_adjoint:
-        large_adj = large_adjoint_block(local, args.large_steps, 20, 4)
+    if world == 1 and not args.no_large_adjoint:
+        large_adj = large_adjoint_block(local, args.large_adjoint_steps, 20, 4)
+    err1000 = None
+    if world == 1 and args.err_steps > 0:
+        err1000 = fp32_error_block(cfg, local, args.err_steps)
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(cfg, 2)
@@ -509,11 +574,16 @@ def main():
         "config": run_config(cfg, world), "fields": 4,
         "path": "FP32 fused path, 4 fields; the FP64 plain path (5 fields) is reported under fp64",
         "fp64": {"value": value64, "ms_per_step": ms64 / args.steps, "fields": 5,
-                 "fp32_speedup": value / value64,
+                 "fp32_speedup": value / value64, "e2e": e2e64,
                  "stage_ms": kt64["stage_ms"], "filter_ms": kt64["filter_ms"], "edge_ms": kt64["edge_ms"]},
         "fp32_rel_err_vs_fp64": err,
+        "fp32_err_c2_1000": err1000,
         "roofline": {"bound": "hbm", "achieved": stage_gbs, "peak": peak, "unit": "GB/s",
                      "frac": stage_gbs / peak, "traffic": stage_traffic(cfg, tile32), "peak_kind": peak_kind,
+                     "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum per stage launch, mean of "
+                                       "the five stages, from the committed ncu launch list of this workload "
+                                       "(profiles/launch_list_c2_6x128cubed.md), not measured in this run",
+                     "timing": "mean per-launch CUDA-event time of launches made without the step graph",
                      "kernel": "stage_kernel<float> (tile x, tile y, planes per CTA = %s)" % (tile32,),
                      "algorithmic_bytes_per_launch": stage_bytes,
                      "mean_launch_ms": kt["stage_ms"],
