@@ -237,7 +237,7 @@ void setup_lagrange(oracle_ctx& c) {
   }
 }
 
-// ic_acoustic_wave.f90:224-272  SOLAR_DATA normalisation by row 1
+// ic_acoustic_wave.f90:61-108  SOLAR_DATA: read the model rows, normalise by row 1
 void solar_data(oracle_ctx& c, const double* model) {
   const int nr = c.nr;
   auto data = [&](int k, int col) { return model[(size_t)(k - 1) * 8 + (col - 1)]; };

@@ -1,8 +1,8 @@
 """Synthetic inputs for the solver's benchmark workloads.
 
 The reference reads its background from a file ``solar_model`` (nr rows of
-r/R, c, rho, p, T, g, Gamma, unused; ic_acoustic_wave.f90:224-229) and
-normalises it by its first row (ic_acoustic_wave.f90:236-271).  It seeds its
+r/R, c, rho, p, T, g, Gamma, unused; ic_acoustic_wave.f90:61-66) and
+normalises it by its first row (ic_acoustic_wave.f90:73-108).  It seeds its
 state with ``GENERATE_IC`` (ic_acoustic_wave.f90:4-29), a plug-in slot selected at
 link time (makefile:16).  Neither the model file nor a public dataset exists
 here, so this module builds seeded synthetic ``solar_model`` tables and source
@@ -36,7 +36,7 @@ from typing import List, Optional, Tuple
 
 import numpy as np
 
-RSUN = 695.9894e8  # ic_acoustic_wave.f90:239
+RSUN = 695.9894e8  # ic_acoustic_wave.f90:76
 
 
 @dataclass
@@ -123,7 +123,7 @@ def model_stratified(nr: int, rmin: float = 0.7, rmax: float = 1.0) -> np.ndarra
 
 
 def normalise(model: np.ndarray):
-    """SOLAR_DATA (ic_acoustic_wave.f90:236-271): background normalised by row 1.
+    """SOLAR_DATA (ic_acoustic_wave.f90:73-108): background normalised by row 1.
 
     Returns (gr, c2, rho0, g0) as float64 arrays of length nr."""
     dimc = model[0, 1]

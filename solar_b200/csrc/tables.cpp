@@ -71,7 +71,7 @@ int build_tables(const solar_desc& d, HostTables& t, std::string& err) {
   t.n = n; t.nr = nr;
   const double pi = std::acos(-1.0);
 
-  // SOLAR_DATA (ic_acoustic_wave.f90:236-271): normalise by the first row.
+  // SOLAR_DATA (ic_acoustic_wave.f90:73-108): normalise by the first row.
   const double* M = d.model;
   const double dimc = M[1], dimrho = M[2], diml = 695.9894e8;
   t.dimc = dimc;
