@@ -173,16 +173,17 @@ int solar_gpu_rk4_norms(solar_ctx* c, int run, int field, int nsteps, double* no
 int solar_gpu_set_watchdog(solar_ctx* c, int every);
 
 /* Failure-detection test hook.  No counterpart in the reference.  Every wait of a
- * streaming kernel on its shared-memory load ring is bounded (one second); a kernel whose
- * wait gives up stops issuing loads, waits (bounded) for the loads it issued, exits, and
- * the call returns SOLAR_ERR_TIMEOUT.  With kernels != 0 the named kernels issue no loads
- * at all and wait at most wait_us microseconds, so their first wait gives up with nothing
- * in flight; kernels = 0 restores normal operation.  Captured step graphs are rebuilt. */
+ * streaming kernel on its shared-memory load ring is bounded (2^22 polls of
+ * mbarrier.try_wait, about a second or more); a kernel whose wait gives up stops issuing
+ * loads, waits (bounded) for the loads it issued, exits, and the call returns
+ * SOLAR_ERR_TIMEOUT.  With kernels != 0 the named kernels issue no loads at all and give up
+ * after `polls` polls (1 .. 2^22), so their first wait runs out with nothing in flight;
+ * kernels = 0 restores normal operation.  Captured step graphs are rebuilt. */
 #define SOLAR_KERNEL_EDGE 1
 #define SOLAR_KERNEL_STAGE 2
 #define SOLAR_KERNEL_FILTER 4
 #define SOLAR_KERNEL_ADJ_STAGE 8
-int solar_gpu_inject_wait_timeout(solar_ctx* c, int kernels, int wait_us);
+int solar_gpu_inject_wait_timeout(solar_ctx* c, int kernels, int polls);
 
 /* FP64 diagnostics of one run: out[0] = acoustic energy
  * 1/2 sum (rho0 |v|^2 + p^2 / (rho0 c^2)) dV, out[1] = sum rho dV, out[2] = max |p|,

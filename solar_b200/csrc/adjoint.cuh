@@ -338,7 +338,7 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const __grid_cons
     }
   }
   // a wait gave up: wait (bounded) for the loads still in flight before the CTA exits
-  if (failed && tid == 0) mbar_drain(bars, L::RING, m_lo, m_seen, m_issued, a.wc.ns);
+  if (failed && tid == 0) mbar_drain(bars, L::RING, m_lo, m_seen, m_issued, a.wc.polls);
 }
 
 // The one-sided radial rows 1, 2 (onto planes 0..6) and nr-3, nr-2 (onto planes nr-7..nr-1)

@@ -327,13 +327,18 @@ __global__ void __launch_bounds__(384, (EdgeMinBlocks<T>::value)) edge_kernel(co
   if (tid == 0 && !a.wc.no_loads)
     for (int d = 0; d < kEdgeDepth && d < kc; ++d) issue(d, d);
   bool ok = mbar_wait(bars, 0, a.wc, kErrEdgeRing), failed = false;
-  int fail_at = ok ? kc : 0;
+  if (__syncthreads_or(!ok)) {
+    // thread 0 issued the first kEdgeDepth planes and saw plane 0 land if its wait succeeded
+    if (tid == 0 && !a.wc.no_loads) mbar_drain(bars, kEdgeRing, 0, ok ? 1 : 0, min(kEdgeDepth, kc), a.wc.polls);
+    return;
+  }
   spread(0, 0);
+  int fail_at = kc;
+  int kk = 0;
   int rs = 0;                                            // ring slot of plane kk
   int ws = kEdgeDepth;                                   // ring slot of plane kk + kEdgeDepth
   int ns = 1;                                            // ring slot of plane kk + 1 ...
   uint32_t np = 0;                                       // ... and the parity of its phase
-  int kk = 0;
   for (; kk < kc; ++kk) {
     if (tid == 0 && ok && !a.wc.no_loads && kk + kEdgeDepth < kc) issue(kk + kEdgeDepth, ws);
     ws = ws + 1 == kEdgeRing ? 0 : ws + 1;
@@ -384,12 +389,12 @@ __global__ void __launch_bounds__(384, (EdgeMinBlocks<T>::value)) edge_kernel(co
     ns = ns + 1 == kEdgeRing ? 0 : ns + 1;
   }
   if (failed) {
-    // thread 0 issued planes [0, issued): up to kk + kEdgeDepth at the break, or only the
-    // first kEdgeDepth if its first wait gave up; it saw [0, seen) land
+    // at the break in iteration kk thread 0 had issued planes [0, kk + kEdgeDepth] and seen
+    // [0, seen) land
     if (tid == 0 && !a.wc.no_loads) {
-      const int issued = min(fail_at == 0 ? kEdgeDepth : kk + kEdgeDepth + 1, kc);
+      const int issued = min(kk + kEdgeDepth + 1, kc);
       const int seen = min(fail_at, min(kk + 2, kc));
-      mbar_drain(bars, kEdgeRing, 0, seen, issued, a.wc.ns);
+      mbar_drain(bars, kEdgeRing, 0, seen, issued, a.wc.polls);
     }
     return;
   }
@@ -756,8 +761,8 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __
     // at the break in iteration k: tile planes [kb, min(k + kTile, ke)) were issued and
     // thread 0 saw [kb, k + 1) land unless one of its waits in this iteration gave up
     const bool own_fail = lead_fail != 0x7fffffff || tile_fail;
-    mbar_drain(barL, kLead, m_lo, min(lead_fail, mq), m_issued, a.wc.ns);
-    mbar_drain(barT, kTile, kb, own_fail ? k : k + 1, min(k + kTile, ke), a.wc.ns);
+    mbar_drain(barL, kLead, m_lo, min(lead_fail, mq), m_issued, a.wc.polls);
+    mbar_drain(barT, kTile, kb, own_fail ? k : k + 1, min(k + kTile, ke), a.wc.polls);
   }
 }
 
@@ -840,11 +845,9 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) filter_kernel(const _
   // The previous kernel may still be finishing (programmatic launch): the input is read
   // only after the wait.
   grid_dependency_wait();
-  // planes [ks, issued) have loads issued; thread 0 has seen planes [ks, seen) land
-  int issued = ks, seen = ks;
   const bool loads = !a.wc.no_loads;
   if (tid == 0 && loads)
-    for (; issued < min(ks + kFiltRing, ke); ++issued) issue(issued, issued - ks);
+    for (int k = ks; k < min(ks + kFiltRing, ke); ++k) issue(k, k - ks);
   T* out = a.qout + g.vol(run, face, s) + g.at(0, j0 + ty, i0 + V * cx);
   const T f0 = Coef<T>::filt(0), f1 = Coef<T>::filt(1), f2 = Coef<T>::filt(2), f3 = Coef<T>::filt(3);
   // radial queue of eta-filtered planes; in float the four values of a thread are held as
@@ -861,7 +864,11 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) filter_kernel(const _
   T zero[V];
 #pragma unroll
   for (int q = 0; q < V; ++q) zero[q] = T(0);
+  // A thread whose wait gives up reports it at the CTA barrier after the xi pass; the CTA
+  // leaves the plane loop there, and thread 0 waits for the planes it issued but did not
+  // see land (fail_at = 2 * plane + whether thread 0's own wait on that plane succeeded).
   bool ok = true;
+  int fail_at = 0;
   int slot = 0;
   uint32_t phase = 0;
   for (int kb = ks; kb < ke && ok; kb += 11) {
@@ -869,8 +876,7 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) filter_kernel(const _
     for (int u = 0; u < 11; ++u) {
       const int k = kb + u;
       if (k >= ke) break;
-      ok = mbar_wait(&bars[slot], phase, a.wc, kErrFilterRing);
-      if (ok) seen = k + 1;
+      const bool got = mbar_wait(&bars[slot], phase, a.wc, kErrFilterRing);
       const T* bx = reinterpret_cast<const T*>(smem + slot * L::P_BYTES);
       T* t1 = reinterpret_cast<T*>(smem + kFiltRing * L::P_BYTES + (k & 1) * L::S_BYTES);
       // xi filter of the box rows (columns V*cx .. V*cx+V-1 of the tile)
@@ -893,8 +899,8 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) filter_kernel(const _
         }
         stv(t1 + r * TX + V * cx, v);
       }
-      if (__syncthreads_or(!ok)) { ok = false; break; }
-      if (tid == 0 && loads && k + kFiltRing < ke) { issue(k + kFiltRing, slot); issued = k + kFiltRing + 1; }
+      if (__syncthreads_or(!got)) { ok = false; fail_at = 2 * k + (got ? 1 : 0); break; }
+      if (tid == 0 && loads && k + kFiltRing < ke) issue(k + kFiltRing, slot);
       if (++slot == kFiltRing) { slot = 0; phase ^= 1; }
       // eta filter of this thread's V points (rows ty .. ty+6 of the xi-filtered tile)
       T c[7][V];
@@ -951,7 +957,11 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) filter_kernel(const _
     const int k = m < 5 ? m : nr - 10 + m;
     if (k >= ko0 && k < ko1) stv(out + (long long)k * g.plane, zero);
   }
-  if (!ok && tid == 0) mbar_drain(bars, kFiltRing, ks, seen, issued, a.wc.ns);
+  if (!ok && tid == 0 && loads) {
+    // at the break on plane k, planes [ks, min(k + kFiltRing, ke)) were issued
+    const int k = fail_at >> 1;
+    mbar_drain(bars, kFiltRing, ks, k + (fail_at & 1), min(k + kFiltRing, ke), a.wc.polls);
+  }
 }
 
 // Edge lines exchanged between processes that own different zones: for item q the

@@ -113,7 +113,7 @@ struct solar_ctx {
   int* err = nullptr;          // device words: [0] error code of a bounded wait that gave up,
                                // [1] step at which the watchdog first saw a non-finite value
   int inject_mask = 0;         // failure-injection tests: kernels that issue no loads ...
-  uint32_t inject_ns = 0;      // ... and their wait bound
+  uint32_t inject_polls = 0;   // ... and their wait bound
   int watch_every = 0;         // NaN/Inf watchdog: check the state every N steps (0 = off)
   long long steps_done = 0;    // steps taken by this context (watchdog step numbers)
   double* norm_ring = nullptr; // per-step sums of squares (solar_gpu_rk4_norms)
@@ -202,7 +202,7 @@ static WaitCtl wait_ctl(const solar_ctx* c, int kind) {
   WaitCtl w;
   w.err = c->err;
   const bool inj = (c->inject_mask & kind) != 0;
-  w.ns = inj ? c->inject_ns : kWaitNs;
+  w.polls = inj ? c->inject_polls : kWaitPolls;
   w.no_loads = inj ? 1 : 0;
   return w;
 }
@@ -304,7 +304,7 @@ static int launch_edge(solar_ctx* c, void* buf, int mode, const int* runs) {
   // a tile box side is at most 256 values; each thread spreads at most one row
   if (smem > 200 * 1024 || a.sp > 256 || 2 * a.sp > 3 * a.ts)
     return fail(SOLAR_ERR_ARG, "edge staging window of %d positions is too wide", a.sp);
-  if (!make_map(c, buf, a.sp, 3, &a.mRow) || !make_map(c, buf, 4, a.sp, &a.mCol))
+  if (!make_map(c, buf, a.sp, 3, &a.mRow) || !make_map(c, buf, 4, a.sp, &a.mCol, false))
     return fail(SOLAR_ERR_CUDA, "cuTensorMapEncodeTiled failed");
   a.wc = wait_ctl(c, kInjEdge);
   static bool attr_set = false;
@@ -1136,15 +1136,15 @@ int solar_gpu_set_watchdog(solar_ctx* c, int every) {
   return SOLAR_OK;
 }
 
-int solar_gpu_inject_wait_timeout(solar_ctx* c, int kernels, int wait_us) {
+int solar_gpu_inject_wait_timeout(solar_ctx* c, int kernels, int polls) {
   int rc = check_ctx(c);
   if (rc) return rc;
   if (kernels & ~(SOLAR_KERNEL_EDGE | SOLAR_KERNEL_STAGE | SOLAR_KERNEL_FILTER | SOLAR_KERNEL_ADJ_STAGE))
     return fail(SOLAR_ERR_ARG, "unknown kernel bits 0x%x", kernels);
-  if (kernels && (wait_us < 1 || wait_us > 1000000)) return fail(SOLAR_ERR_ARG, "wait_us must be in 1..1000000");
+  if (kernels && (polls < 1 || polls > (int)kWaitPolls)) return fail(SOLAR_ERR_ARG, "polls must be in 1..%u", kWaitPolls);
   CK(cudaStreamSynchronize(c->stream));
   c->inject_mask = kernels;
-  c->inject_ns = kernels ? (uint32_t)wait_us * 1000u : 0u;
+  c->inject_polls = kernels ? (uint32_t)polls : 0u;
   // the captured step graphs hold the old launch arguments
   if (c->step_graph) { cudaGraphExecDestroy(c->step_graph); c->step_graph = nullptr; }
   drop_batch_graphs(c);

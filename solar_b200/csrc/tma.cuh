@@ -3,8 +3,9 @@
 //
 // Only plain (single-CTA) tile loads are used: every load reads this GPU's own memory.
 //
-// Every wait on an mbarrier is bounded by time (the global nanosecond timer): after the
-// kernel's limit (kWaitNs, one second) the waiting thread gets `false` and records an
+// Every wait on an mbarrier is bounded: after the kernel's limit of polls (kWaitPolls, about
+// a second or more -- each mbarrier.try_wait may suspend the thread for a while before it
+// reports that the phase is still open) the waiting thread gets `false` and records an
 // error code in the context's device error word, which the host turns into
 // SOLAR_ERR_TIMEOUT.  A CTA whose wait gave up stops issuing loads, leaves its plane loop
 // at the next CTA barrier and, before it exits, waits (bounded again) for every load it
@@ -19,7 +20,7 @@
 
 namespace solar {
 
-constexpr uint32_t kWaitNs = 1000000000u;   // bound of one wait: 1 s
+constexpr uint32_t kWaitPolls = 1u << 22;   // bound of one wait: polls of try_wait
 
 // Codes a kernel leaves in the context's device error word.
 enum DeviceError : int {
@@ -35,11 +36,11 @@ enum DeviceError : int {
 enum InjectKernel : int { kInjEdge = 1, kInjStage = 2, kInjFilter = 4, kInjAdjStage = 8 };
 
 // Wait control carried in a kernel's arguments: the device error word, the bound of one
-// wait in nanoseconds, and the injection switch of failure-detection tests (nonzero: the
+// wait in polls, and the injection switch of failure-detection tests (nonzero: the
 // producer issues no loads, so the first wait runs out with nothing in flight).
 struct WaitCtl {
   int* err;
-  uint32_t ns;
+  uint32_t polls;
   int no_loads;
 };
 
@@ -61,37 +62,31 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
                : "memory");
 }
 
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_try_wait_u32(uint32_t bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
       "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
       : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
+      : "r"(bar), "r"(parity)
       : "memory");
   return ok != 0;
 }
 
-__device__ __forceinline__ uint64_t global_ns() {
-  uint64_t t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  return mbar_try_wait_u32(smem_u32(bar), parity);
 }
 
-// Wait at most limit_ns for the phase with the given parity to complete.
-__device__ __forceinline__ bool mbar_wait_ns(uint64_t* bar, uint32_t parity, uint32_t limit_ns) {
-  if (mbar_try_wait(bar, parity)) return true;
-  const uint64_t t0 = global_ns();
-  for (;;) {
-#pragma unroll 1
-    for (int i = 0; i < 32; ++i)
-      if (mbar_try_wait(bar, parity)) return true;
-    if (global_ns() - t0 > limit_ns) return false;
-  }
+// Wait for the phase with the given parity to complete, at most `polls` tests.
+__device__ __forceinline__ bool mbar_wait_polls(uint64_t* bar, uint32_t parity, uint32_t polls) {
+  const uint32_t b = smem_u32(bar);
+  for (uint32_t it = 0; it < polls; ++it)
+    if (mbar_try_wait_u32(b, parity)) return true;
+  return false;
 }
 
 // Consumer wait: on giving up, record `code` in the device error word.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, const WaitCtl& w, int code) {
-  if (mbar_wait_ns(bar, parity, w.ns)) return true;
+  if (mbar_wait_polls(bar, parity, w.polls)) return true;
   if (w.err) atomicExch(w.err, code);
   return false;
 }
@@ -99,10 +94,10 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, const 
 // Before a CTA that gave up exits: wait (bounded) for the loads of planes [first, end) of a
 // ring of `slots` mbarriers filled in plane order from plane `base` (plane m in slot
 // (m - base) % slots, phase parity ((m - base) / slots) & 1).
-__device__ __forceinline__ void mbar_drain(uint64_t* bars, int slots, int base, int first, int end, uint32_t limit_ns) {
+__device__ __forceinline__ void mbar_drain(uint64_t* bars, int slots, int base, int first, int end, uint32_t polls) {
   for (int m = first; m < end; ++m) {
     const int q = m - base;
-    mbar_wait_ns(&bars[q % slots], (uint32_t)((q / slots) & 1), limit_ns);
+    mbar_wait_polls(&bars[q % slots], (uint32_t)((q / slots) & 1), polls);
   }
 }
 

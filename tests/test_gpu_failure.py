@@ -1,8 +1,8 @@
 """Failure detection on the GPU, without faulting, trapping or hanging it.
 
 * Bounded waits: every streaming kernel waits on its shared-memory load ring for at most a
-  fixed time.  The test switch solar_gpu_inject_wait_timeout makes the chosen kernel issue
-  no loads and wait only briefly, so its first wait runs out with nothing in flight; the
+  fixed number of polls.  The test switch solar_gpu_inject_wait_timeout makes the chosen kernel issue
+  no loads and give up after a few polls, so its first wait runs out with nothing in flight; the
   call must return SOLAR_ERR_TIMEOUT naming the kernel, and the same context (and a fresh
   one) must give the correct results afterwards.
 * NaN/Inf watchdog: a non-finite value placed in the host state passed to set_state makes a
@@ -18,7 +18,7 @@ from solar_b200.solver import Solver
 
 pytestmark = pytest.mark.gpu
 
-WAIT_US = 200        # bound of the injected waits
+WAIT_POLLS = 1000    # bound of the injected waits (polls of mbarrier.try_wait)
 
 
 def smooth_state(cfg, seed):
@@ -44,8 +44,8 @@ def q0(cfg):
     return smooth_state(cfg, 7)
 
 
-def inject(s, kernels, wait_us=WAIT_US):
-    _lib.check(s.lib.solar_gpu_inject_wait_timeout(s._h, kernels, wait_us))
+def inject(s, kernels, polls=WAIT_POLLS):
+    _lib.check(s.lib.solar_gpu_inject_wait_timeout(s._h, kernels, polls))
 
 
 CASES = [
