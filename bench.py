@@ -398,10 +398,10 @@ def large_block(device: int, nsteps: int):
 
 
 def split_block(cfg, args, world, local):
-    """Zones split across the job's processes (strong scaling of one six-zone run): each
-    rank owns 6/world zones and exchanges edge lines with its neighbours every phase over
-    torch.distributed (NCCL).  Timed with CUDA events on the library's stream, max over
-    ranks."""
+    """The sphere split across the job's processes (strong scaling of one six-zone run):
+    gcd(world, 6) zone groups x radial slabs; each rank exchanges edge lines and boundary
+    planes with its neighbours every phase over torch.distributed (NCCL).  Timed with CUDA
+    events on the library's stream, max over ranks."""
     import torch
 
     import torch.distributed as dist
@@ -429,8 +429,9 @@ def split_block(cfg, args, world, local):
     zs.close()
     if own_group:
         dist.destroy_process_group()
+    ngroups, nslabs = D.layout(world)
     return {"value": cfg.points * args.steps / (ms / 1e3), "unit": "grid-pt RK4 updates/s", "scaling": "strong",
-            "ms_per_step": ms / args.steps, "zones_per_rank": 6 // world, "norm_vr": norm}
+            "ms_per_step": ms / args.steps, "zone_groups": ngroups, "radial_slabs": nslabs, "norm_vr": norm}
 
 
 def large_adjoint_block(device: int, nsteps: int, outer: int, inner: int):
@@ -479,7 +480,7 @@ def main():
     ap.add_argument("--err-steps", type=int, default=1000,
                     help="steps of the FP32-vs-FP64 error check on the workload (0 = skip)")
     ap.add_argument("--split", action="store_true",
-                    help="also run the zones split across the job's processes (world must divide 6)")
+                    help="also run the sphere split across the job's processes (zone groups x radial slabs)")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-large", action="store_true")
     ap.add_argument("--large-steps", type=int, default=200)

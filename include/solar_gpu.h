@@ -244,8 +244,29 @@ int solar_gpu_edge_routes(int* routes);
 /* One phase of an RK4 call, enqueued on the context's stream (no wait): phases 0..4 are
  * the five stages (edge exchange of p, v_xi, v_eta + fused stage kernel), phase 5 is
  * FILTER_EXP (edge exchange of every field + filter).  Phases 0..5 in order = one
- * solar_gpu_rk4(c, 1). */
+ * solar_gpu_rk4(c, 1).  Phases 6 and 7 are the two halves of phase 5 (edge exchange; filter),
+ * between which a process owning a radial slab receives its neighbours' boundary planes. */
 int solar_gpu_step_phase(solar_ctx* c, int phase);
+
+/* ---- Radial slabs (the reference's pr decomposition, header:6; nruns == 1) -------------
+ * The step kernels compute planes k0 .. k1-1 only (k1 - k0 >= 5; default 0 .. nr-1).  The
+ * radial stencils near a slab boundary read the neighbouring slab's planes, which the host
+ * moves between the phases of a step (derivative.f90:605-758 exchanges 3 planes for DDR,
+ * filter.f90:633-781 5 planes for FILTER_R): before stage phase p (0..4) the 3 planes of p and
+ * v_r next to each boundary, before the filter (between phases 6 and 7) the 5 planes of every
+ * stored field, frames included.  Zones and slabs combine: a process owns a zone range and a
+ * plane range; the edge lines of solar_gpu_pack_lines then cover the owned planes only. */
+int solar_gpu_set_owned_planes(solar_ctx* c, int k0, int k1);
+
+/* Values (of the context's precision) one phase sends to one radial neighbour: owned zones x
+ * fields (2 before a stage, nfields before the filter) x planes (3 / 5) x padded plane. */
+long long solar_gpu_planes_size(solar_ctx* c, int phase);
+
+/* side 0: the neighbour below (sends planes k0 .. k0+H-1, receives k0-H .. k0-1);
+ * side 1: the neighbour above (sends k1-H .. k1-1, receives k1 .. k1+H-1).  phase 0..5 names
+ * the exchange (5 = the filter's).  Enqueued on the context's stream. */
+int solar_gpu_pack_planes(solar_ctx* c, int phase, int side, void* d_buf);
+int solar_gpu_unpack_planes(solar_ctx* c, int phase, int side, const void* d_buf);
 
 /* Values (of the context's precision) in the packed lines of one (zone, edge) pair in
  * phase `phase`: 3 * nx * nr * (3 fields in phases 0..4, every stored field in phase 5). */

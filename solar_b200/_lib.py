@@ -91,6 +91,10 @@ EXPORTS = {
     "solar_gpu_set_owned_zones": [_P, ctypes.c_int, ctypes.c_int],
     "solar_gpu_edge_routes": [_I],
     "solar_gpu_step_phase": [_P, ctypes.c_int],
+    "solar_gpu_set_owned_planes": [_P, ctypes.c_int, ctypes.c_int],
+    "solar_gpu_planes_size": [_P, ctypes.c_int],
+    "solar_gpu_pack_planes": [_P, ctypes.c_int, ctypes.c_int, ctypes.c_void_p],
+    "solar_gpu_unpack_planes": [_P, ctypes.c_int, ctypes.c_int, ctypes.c_void_p],
     "solar_gpu_lines_size": [_P, ctypes.c_int],
     "solar_gpu_pack_lines": [_P, ctypes.c_int, _I, ctypes.c_int, ctypes.c_void_p],
     "solar_gpu_unpack_lines": [_P, ctypes.c_int, _I, ctypes.c_int, ctypes.c_void_p],
@@ -119,6 +123,7 @@ EXPORTS = {
 
 # entry points whose return type is not int
 RESTYPES = {"solar_desc_defaults": None, "solar_gpu_lines_size": ctypes.c_longlong,
+            "solar_gpu_planes_size": ctypes.c_longlong,
             "solar_gpu_stream": ctypes.c_void_p}
 
 _lib = None

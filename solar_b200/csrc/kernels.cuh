@@ -36,6 +36,7 @@ struct Geom {
   int nruns;
   int slot[5];              // slot of each reference field, -1 if not stored
   int face0, nface;         // zones the step kernels work on (a process owning part of the sphere)
+  int k0, k1;               // radial planes the step kernels compute (a process owning a radial slab)
   __host__ __device__ long long vol(int run, int face, int s) const {
     return ((long long)(run * 6 + face) * nf + s) * vs;
   }
@@ -196,9 +197,9 @@ __global__ void __launch_bounds__(384, (EdgeMinBlocks<T>::value)) edge_kernel(co
   const int n = g.n, ts = a.ts, sp = a.sp;
   // the run map is written before the launches that use it and constant during them
   const int run = a.runs ? a.runs[blockIdx.z] : blockIdx.z;
-  const int kb = blockIdx.x * a.kchunk;
-  if (kb >= g.nr) return;
-  const int kc = min(a.kchunk, g.nr - kb);
+  const int kb = g.k0 + blockIdx.x * a.kchunk;
+  if (kb >= g.k1) return;
+  const int kc = min(a.kchunk, g.k1 - kb);
   int y = blockIdx.y;
   const int seg = y % a.nseg;
   y /= a.nseg;
@@ -493,9 +494,9 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __
   // the run map is written before the launches that use it and constant during them
   const int zr = blockIdx.z / g.nface;
   const int run = a.runs ? a.runs[zr] : zr, face = g.face0 + blockIdx.z % g.nface;
-  const int kb = blockIdx.y * a.kchunk;
-  if (kb >= nr) return;
-  const int ke = min(nr, kb + a.kchunk);
+  const int kb = g.k0 + blockIdx.y * a.kchunk;
+  if (kb >= g.k1) return;
+  const int ke = min(g.k1, kb + a.kchunk);
   const int cx = threadIdx.x, ty = threadIdx.y, tid = ty * NT + cx;
   const int sP = g.slot[kP], sX = g.slot[kVxi], sY = g.slot[kVeta], sR = g.slot[kVr], sRho = g.slot[kRho];
   const int zbase = (run * 6 + face) * g.nf;   // plane index of (slot s, k) = (zbase + s) * nr + k
@@ -815,12 +816,12 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) filter_kernel(const _
   const int tiles_x = n / TX, tiles = tiles_x * (n / TY);
   // unit = (tile, stored field, run and owned face); whole units first, then the radial
   // chunks of the remaining units (output planes [ko0, ko1), input planes [ks, ke))
-  int unit = blockIdx.x, ko0 = 0, ko1 = nr;
+  int unit = blockIdx.x, ko0 = g.k0, ko1 = g.k1;
   if (unit >= a.whole) {
-    const int t = unit - a.whole, c = t % a.chunks;
+    const int t = unit - a.whole, c = t % a.chunks, nk = g.k1 - g.k0;
     unit = a.whole + t / a.chunks;
-    ko0 = c * nr / a.chunks;
-    ko1 = (c + 1) * nr / a.chunks;
+    ko0 = g.k0 + c * nk / a.chunks;
+    ko1 = g.k0 + (c + 1) * nk / a.chunks;
   }
   const int ks = max(0, ko0 - 5), ke = min(nr, ko1 + 5);
   const int tile = unit % tiles, rest = unit / tiles;
@@ -967,7 +968,8 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) filter_kernel(const _
 // Edge lines exchanged between processes that own different zones: for item q the
 // (zone, edge) pair items[2q], items[2q+1]; the three lines next to that edge that the
 // neighbouring zone interpolates from (rows 1..3 / n-2..n-4, columns likewise), for the
-// slots listed in `slots`.  Packed layout [item][slot][k][layer][t], t along the edge.
+// slots listed in `slots`, over the owned planes k0 .. k1-1.  Packed layout
+// [item][slot][k - k0][layer][t], t along the edge.
 template <typename T>
 __device__ __forceinline__ long long line_offset(const Geom& g, int face, int e, int s, int k, int l, int t) {
   const int n = g.n;
@@ -982,13 +984,14 @@ __device__ __forceinline__ long long line_offset(const Geom& g, int face, int e,
 template <typename T>
 __global__ void line_pack_kernel(const T* __restrict__ q, T* __restrict__ out, const int* __restrict__ items,
                                  int nitems, const int* __restrict__ slots, int nslots, Geom g, int unpack) {
-  const long long per = (long long)3 * g.n * g.nr;          // one slot of one item
+  const int nk = g.k1 - g.k0;                                // owned planes
+  const long long per = (long long)3 * g.n * nk;             // one slot of one item
   const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= per * nslots * nitems) return;
   const int t = idx % g.n;
   long long r = idx / g.n;
   const int l = r % 3; r /= 3;
-  const int k = r % g.nr; r /= g.nr;
+  const int k = g.k0 + (int)(r % nk); r /= nk;
   const int si = r % nslots;
   const int it = (int)(r / nslots);
   const long long o = line_offset<T>(g, items[2 * it], items[2 * it + 1], slots[si], k, l, t);
@@ -1068,7 +1071,8 @@ __global__ void gaussian_kernel(double* p, Geom g, int face, const double* tanx,
 template <typename T>
 __global__ void sumsq_plane_kernel(const T* __restrict__ q, Geom g, int run, int slot, double* part) {
   constexpr int V = Vec16<T>::V;
-  const int face = g.face0 + blockIdx.x / g.nr, k = blockIdx.x % g.nr;
+  const int nk = g.k1 - g.k0;
+  const int face = g.face0 + blockIdx.x / nk, k = g.k0 + blockIdx.x % nk;
   const int n = g.n, per_row = n / V;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
   const T* base = q + g.vol(run, face, slot) + g.at(k, 0, 0);
@@ -1138,7 +1142,8 @@ template <typename T>
 __global__ void reduce_plane_kernel(const T* q, Geom g, int run, int sel_slot, const double* rad64,
                                     const double* vol2, const double* drw, const double* c2_3d,
                                     double* part) {
-  const int face = g.face0 + blockIdx.x / g.nr, k = blockIdx.x % g.nr;
+  const int nk = g.k1 - g.k0;
+  const int face = g.face0 + blockIdx.x / nk, k = g.k0 + blockIdx.x % nk;
   const int n = g.n;
   double acc[5] = {0, 0, 0, 0, 0};
   const double rho0 = rad64[rRho0 * g.nr + k];

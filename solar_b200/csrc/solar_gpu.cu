@@ -299,7 +299,8 @@ static int launch_edge(solar_ctx* c, void* buf, int mode, const int* runs) {
   const long long per_chunk = 4LL * c->g.nface * a.ngroups * a.nseg * nrl;
   const long long slots = (long long)c->nsm * EdgeMinBlocks<T>::value;
   const long long nch = std::max<long long>(1, slots / per_chunk);
-  a.kchunk = std::max<int>(4, (int)((c->g.nr + nch - 1) / nch));
+  const int nk = c->g.k1 - c->g.k0;
+  a.kchunk = std::max<int>(4, (int)((nk + nch - 1) / nch));
   const size_t smem = (size_t)edge_smem_bytes(a.sp, a.ts, (int)sizeof(T));
   // a tile box side is at most 256 values; each thread spreads at most one row
   if (smem > 200 * 1024 || a.sp > 256 || 2 * a.sp > 3 * a.ts)
@@ -312,7 +313,7 @@ static int launch_edge(solar_ctx* c, void* buf, int mode, const int* runs) {
     CK(cudaFuncSetAttribute(edge_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     attr_set = true;
   }
-  dim3 grid((c->g.nr + a.kchunk - 1) / a.kchunk, 4 * c->g.nface * a.ngroups * a.nseg, nrl);
+  dim3 grid((nk + a.kchunk - 1) / a.kchunk, 4 * c->g.nface * a.ngroups * a.nseg, nrl);
   CK(launch_pdl(edge_kernel<T>, grid, dim3(3 * a.ts), smem, c->stream, a));
   return SOLAR_OK;
 }
@@ -330,7 +331,7 @@ static int launch_stage_t(solar_ctx* c, StageArgs<T>& a, const void* qin) {
                             (int)L::TOTAL));
     attr_set = true;
   }
-  const int nchunks = (c->g.nr + a.kchunk - 1) / a.kchunk;
+  const int nchunks = (c->g.k1 - c->g.k0 + a.kchunk - 1) / a.kchunk;
   dim3 grid((c->g.n / TX) * (c->g.n / TY), nchunks, launched_runs(c, a.runs) * c->g.nface);
   CK(launch_pdl(stage_kernel<T, TX, TY, MODE, HAS_RHO, FORCE>, grid, dim3(TX / Vec16<T>::V, TY), L::TOTAL, c->stream, a));
   return SOLAR_OK;
@@ -425,7 +426,7 @@ static int launch_filter_t(solar_ctx* c, const void* qin, void* qout, const int*
   a.whole = (int)units;
   a.chunks = 1;
   if (units > slots && tail > 0) {
-    const int chunks = (int)std::min<long long>(c->g.nr / 11, std::max<long long>(1, (slots + tail / 2) / tail));
+    const int chunks = (int)std::min<long long>((c->g.k1 - c->g.k0) / 11, std::max<long long>(1, (slots + tail / 2) / tail));
     if (chunks > 1) {
       a.whole = (int)(units - tail);
       a.chunks = chunks;
@@ -619,7 +620,7 @@ static int check_ctx(solar_ctx* c) {
 }
 
 static int reduce(solar_ctx* c, int run, int sel_field, double* out5) {
-  const int nblocks = c->g.nface * c->g.nr;
+  const int nblocks = c->g.nface * (c->g.k1 - c->g.k0);
   const int sel = (sel_field >= 0 && sel_field < 5) ? c->g.slot[sel_field] : -1;
   if (c->fp32)
     reduce_plane_kernel<float><<<nblocks, 256, 0, c->stream>>>((const float*)c->A, c->g, run, sel, c->dt.rad64,
@@ -640,7 +641,7 @@ static int reduce(solar_ctx* c, int run, int sel_field, double* out5) {
 static int sumsq(solar_ctx* c, int run, int sel_field, double* out) {
   const int s = c->g.slot[sel_field];
   if (s < 0) { *out = 0.0; return SOLAR_OK; }
-  const int nblocks = c->g.nface * c->g.nr;
+  const int nblocks = c->g.nface * (c->g.k1 - c->g.k0);
   if (c->fp32) sumsq_plane_kernel<float><<<nblocks, 256, 0, c->stream>>>((const float*)c->A, c->g, run, s, c->part);
   else sumsq_plane_kernel<double><<<nblocks, 256, 0, c->stream>>>((const double*)c->A, c->g, run, s, c->part);
   CK(cudaGetLastError());
@@ -741,6 +742,8 @@ int solar_gpu_init(const solar_desc* d, solar_ctx** out) {
   g.nruns = d->nruns;
   g.face0 = 0;
   g.nface = 6;
+  g.k0 = 0;
+  g.k1 = g.nr;
   if (g.nf == 5) { for (int f = 0; f < 5; ++f) g.slot[f] = f; }
   else { g.slot[kRho] = -1; g.slot[kVxi] = 0; g.slot[kVeta] = 1; g.slot[kVr] = 2; g.slot[kP] = 3; }
   // tile choice (16x16, 32x8, 32x16, 64x8)
@@ -1109,7 +1112,7 @@ int solar_gpu_rk4_norms(solar_ctx* c, int run, int field, int nsteps, double* no
   }
   if ((rc = capture_step_graph(c))) return rc;
   const int slot = c->g.slot[field - 1];
-  const int nblocks = c->g.nface * c->g.nr;
+  const int nblocks = c->g.nface * (c->g.k1 - c->g.k0);
   if (slot < 0) CK(cudaMemsetAsync(c->norm_ring, 0, (size_t)nsteps * sizeof(double), c->stream));
   for (int s = 0; s < nsteps; ++s) {
     CK(cudaGraphLaunch(c->step_graph, c->stream));

@@ -42,7 +42,7 @@ static int lines_op(solar_ctx* c, int phase, const int* zone_edge, int count, vo
   if (!count) return SOLAR_OK;
   const int ns = phase_slots(c, phase);
   const int* slots = c->split_slots + (phase == 5 ? 3 : 0);
-  const long long total = 3LL * c->g.n * c->g.nr * ns * count;
+  const long long total = 3LL * c->g.n * (c->g.k1 - c->g.k0) * ns * count;
   const unsigned blocks = (unsigned)((total + 255) / 256);
   void* q = phase_buffer(c, phase);
   if (c->fp32)
@@ -55,6 +55,9 @@ static int lines_op(solar_ctx* c, int phase, const int* zone_edge, int count, vo
   return SOLAR_OK;
 }
 
+// Phases 0..4: edge exchange + stage s; 5: edge exchange + FILTER_EXP; 6 and 7: the two
+// halves of phase 5 (a process owning a radial slab receives its neighbours' boundary
+// planes, frames included, between them).
 template <typename T>
 static int enqueue_phase(solar_ctx* c, int phase) {
   int rc;
@@ -65,9 +68,51 @@ static int enqueue_phase(solar_ctx* c, int phase) {
     if ((rc = launch_edge<T>(c, in, 0, nullptr))) return rc;
     return launch_stage<T>(c, in, out, phase == 0 ? 1 : 0, phase, nullptr);
   }
-  if ((rc = launch_edge<T>(c, c->B, 1, nullptr))) return rc;
+  if (phase != 7 && (rc = launch_edge<T>(c, c->B, 1, nullptr))) return rc;
+  if (phase == 6) return SOLAR_OK;
   if ((rc = launch_filter<T>(c, c->B, c->A, nullptr))) return rc;
   return force_end(c);
+}
+
+// Boundary planes exchanged between radial slabs: before stage s the three planes of p and
+// v_r next to each slab boundary (the 7-point radial windows), before FILTER_EXP the five
+// planes of every stored field (the 11-point radial filter; sent after the edge exchange,
+// so with their frames).  Whole padded planes of the owned zones, [zone][field][plane].
+static int halo_planes(int phase) { return phase == 5 ? 5 : 3; }
+static int halo_fields(const solar_ctx* c, int phase, int* slots) {
+  if (phase == 5) {
+    for (int s = 0; s < c->g.nf; ++s) slots[s] = s;
+    return c->g.nf;
+  }
+  slots[0] = c->g.slot[kP];
+  slots[1] = c->g.slot[kVr];
+  return 2;
+}
+
+static int planes_op(solar_ctx* c, int phase, int side, void* d_buf, int unpack) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (phase < 0 || phase > 5 || side < 0 || side > 1) return fail(SOLAR_ERR_ARG, "phase must be 0..5, side 0 or 1");
+  if (c->g.nruns != 1) return fail(SOLAR_ERR_ARG, "radial slabs need nruns == 1");
+  if (!d_buf) return fail(SOLAR_ERR_ARG, "null device buffer");
+  const Geom& g = c->g;
+  const int H = halo_planes(phase);
+  if (side == 0 ? g.k0 < H : g.k1 + H > g.nr) return fail(SOLAR_ERR_ARG, "no radial neighbour on side %d", side);
+  int slots[5];
+  const int nfld = halo_fields(c, phase, slots);
+  // sent: the owned planes next to the boundary; received: the planes just outside it
+  const int k = unpack ? (side == 0 ? g.k0 - H : g.k1) : (side == 0 ? g.k0 : g.k1 - H);
+  unsigned char* buf = static_cast<unsigned char*>(phase_buffer(c, phase));
+  unsigned char* dev = static_cast<unsigned char*>(d_buf);
+  const size_t block = (size_t)H * g.plane * c->esize;
+  size_t off = 0;
+  for (int f = g.face0; f < g.face0 + g.nface; ++f)
+    for (int q = 0; q < nfld; ++q, off += block) {
+      unsigned char* vol = buf + (size_t)(g.vol(0, f, slots[q]) + (long long)k * g.plane) * c->esize;
+      if (unpack) CK(cudaMemcpyAsync(vol, dev + off, block, cudaMemcpyDeviceToDevice, c->stream));
+      else CK(cudaMemcpyAsync(dev + off, vol, block, cudaMemcpyDeviceToDevice, c->stream));
+    }
+  return SOLAR_OK;
 }
 
 }  // namespace solar
@@ -102,16 +147,45 @@ int solar_gpu_edge_routes(int* routes) {
 int solar_gpu_step_phase(solar_ctx* c, int phase) {
   int rc = check_ctx(c);
   if (rc) return rc;
-  if (phase < 0 || phase > 5) return fail(SOLAR_ERR_ARG, "phase must be 0..5");
+  if (phase < 0 || phase > 7) return fail(SOLAR_ERR_ARG, "phase must be 0..7");
   rc = c->fp32 ? enqueue_phase<float>(c, phase) : enqueue_phase<double>(c, phase);
   if (rc) return rc;
   CK(cudaGetLastError());
-  return phase == 5 ? watch_after_step(c) : SOLAR_OK;
+  return (phase == 5 || phase == 7) ? watch_after_step(c) : SOLAR_OK;
+}
+
+int solar_gpu_set_owned_planes(solar_ctx* c, int k0, int k1) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  const int nr = c->g.nr;
+  if (k0 < 0 || k1 > nr || k1 - k0 < 5) return fail(SOLAR_ERR_ARG, "owned planes [%d, %d) must lie in 0..%d and hold >= 5 planes", k0, k1, nr);
+  if (c->g.nruns != 1 && (k0 != 0 || k1 != nr)) return fail(SOLAR_ERR_ARG, "radial slabs need nruns == 1");
+  CK(cudaStreamSynchronize(c->stream));
+  c->g.k0 = k0;
+  c->g.k1 = k1;
+  // captured graphs hold the old launch shapes
+  if (c->step_graph) { cudaGraphExecDestroy(c->step_graph); c->step_graph = nullptr; }
+  drop_batch_graphs(c);
+  return SOLAR_OK;
+}
+
+long long solar_gpu_planes_size(solar_ctx* c, int phase) {
+  if (!c || phase < 0 || phase > 5) return -1;
+  int slots[5];
+  return (long long)c->g.nface * halo_fields(c, phase, slots) * halo_planes(phase) * c->g.plane;
+}
+
+int solar_gpu_pack_planes(solar_ctx* c, int phase, int side, void* d_buf) {
+  return planes_op(c, phase, side, d_buf, 0);
+}
+
+int solar_gpu_unpack_planes(solar_ctx* c, int phase, int side, const void* d_buf) {
+  return planes_op(c, phase, side, const_cast<void*>(d_buf), 1);
 }
 
 long long solar_gpu_lines_size(solar_ctx* c, int phase) {
   if (!c || phase < 0 || phase > 5) return -1;
-  return 3LL * c->g.n * c->g.nr * phase_slots(c, phase);
+  return 3LL * c->g.n * (c->g.k1 - c->g.k0) * phase_slots(c, phase);
 }
 
 int solar_gpu_pack_lines(solar_ctx* c, int phase, const int* zone_edge, int count, void* d_buf) {

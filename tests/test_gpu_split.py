@@ -1,11 +1,12 @@
-"""Zones split across processes, on one GPU.
+"""The sphere split across processes, on one GPU.
 
-Each emulated rank is its own context owning partition(world)[rank] zones; the ranks are
-stepped phase by phase from one host thread, with the edge lines of every phase packed by
-the library, copied between the ranks' buffers and unpacked (no kernel waits on another).
-The assembled owned zones must equal the single-context run bit for bit: the split path
-runs the same kernels on the same inputs.  A one-rank NCCL process group also runs the
-torch.distributed path (ZoneSplitSolver) end to end.
+Each emulated rank is its own context owning a zone range (and, for 4 and 8 ranks, a radial
+slab: 2 zone groups x 2 or 4 slabs); the ranks are stepped phase by phase from one host
+thread, with the edge lines and boundary planes of every phase packed by the library,
+copied between the ranks' buffers and unpacked (no kernel waits on another).  The assembled
+owned parts must equal the single-context run bit for bit: the split path runs the same
+kernels on the same inputs.  A one-rank NCCL process group also runs the torch.distributed
+path (ZoneSplitSolver) end to end.
 """
 import os
 import socket
@@ -88,6 +89,113 @@ def test_split_run_equals_single_context(cfg, world, precision, nfields):
     assert abs(norm - want_norm) <= 1e-12 * want_norm
 
 
+def emulate_slabs(cfg, world, nsteps, q0, precision, nfields):
+    """World ranks laid out as D.layout(world) zone groups x radial slabs, one context each."""
+    import ctypes
+
+    import torch
+    ngroups, nsl = D.layout(world)
+    dtype = torch.float32 if precision == "fp32" else torch.float64
+    alloc = lambda n: torch.zeros(n, dtype=dtype, device="cuda")
+    ranks = []
+    try:
+        for r in range(world):
+            zg, sl = divmod(r, nsl)
+            z0, nz = D.partition(ngroups)[zg]
+            k0, k1 = D.slabs(cfg.nr, nsl)[sl]
+            s = Solver(cfg, precision=precision, nfields=nfields)
+            s.set_state(q0)
+            _lib.check(s.lib.solar_gpu_set_owned_zones(s._h, z0, nz))
+            _lib.check(s.lib.solar_gpu_set_owned_planes(s._h, k0, k1))
+            plan, below, above = D.slab_plan(world, r)
+            lx = D.LineExchange(plan, D._LibPacker(s), None, alloc)
+            px = D.PlaneExchange(below, above, D._LibPlanePacker(s), None, alloc)
+            ranks.append((s, lx, px, (z0, nz, k0, k1)))
+
+        def lines(phase):
+            for s, lx, _, _ in ranks:
+                lx.pack(phase)
+            for s, _, _, _ in ranks:
+                s.synchronize()
+            for r, (_, lx, _, _) in enumerate(ranks):
+                for peer, buf in lx.buffers(phase)[1].items():
+                    buf.copy_(ranks[peer][1].buffers(phase)[0][r])
+            torch.cuda.synchronize()
+            for _, lx, _, _ in ranks:
+                lx.unpack(phase)
+
+        def planes(phase):
+            for _, _, px, _ in ranks:
+                px.pack(phase)
+            for s, _, _, _ in ranks:
+                s.synchronize()
+            for r, (_, _, px, _) in enumerate(ranks):
+                for side, buf in px.buffers(phase)[1].items():
+                    peer = px.peers[side]
+                    buf.copy_(ranks[peer][2].buffers(phase)[0][1 - side])   # the peer's send toward me
+            torch.cuda.synchronize()
+            for _, _, px, _ in ranks:
+                px.unpack(phase)
+
+        def step(phase):
+            for s, _, _, _ in ranks:
+                _lib.check(s.lib.solar_gpu_step_phase(s._h, phase))
+
+        for _ in range(nsteps):
+            for phase in range(5):
+                lines(phase)
+                planes(phase)
+                step(phase)
+            lines(5)
+            step(6)
+            planes(5)
+            step(7)
+        q = np.zeros_like(q0)
+        sumsq = 0.0
+        for s, _, _, (z0, nz, k0, k1) in ranks:
+            q[z0:z0 + nz, :, k0:k1] = s.get_state()[z0:z0 + nz, :, k0:k1]
+            out = (ctypes.c_double * 5)()
+            _lib.check(s.lib.solar_gpu_reduce_owned(s._h, 0, 4, out))
+            sumsq += out[0]
+        return q, sumsq
+    finally:
+        for s, _, _, _ in ranks:
+            s.close()
+
+
+@pytest.mark.parametrize("world", [4, 8])
+@pytest.mark.parametrize("precision,nfields", [("fp64", 5), ("fp32", 4)])
+def test_zone_and_slab_split_equals_single_context(cfg, world, precision, nfields):
+    q0 = initial_state(cfg)
+    nsteps = 5
+    with Solver(cfg, precision=precision, nfields=nfields) as s:
+        s.set_state(q0)
+        s.rk4(nsteps)
+        want = s.get_state()
+        want_norm = s.norm(4)
+    got, sumsq = emulate_slabs(cfg, world, nsteps, q0, precision, nfields)
+    np.testing.assert_array_equal(got, want)
+    norm = (sumsq / (cfg.nx * cfg.nx * cfg.nr) * 6.0) ** 0.5
+    assert abs(norm - want_norm) <= 1e-12 * want_norm
+
+
+def test_plane_exchange_arguments(cfg):
+    import ctypes
+
+    import torch
+    with Solver(cfg) as s:
+        assert s.lib.solar_gpu_set_owned_planes(s._h, 0, 4) == _lib.SOLAR_ERR_ARG      # fewer than 5 planes
+        assert s.lib.solar_gpu_set_owned_planes(s._h, 10, cfg.nr + 1) == _lib.SOLAR_ERR_ARG
+        _lib.check(s.lib.solar_gpu_set_owned_planes(s._h, 0, 16))
+        n = s.lib.solar_gpu_planes_size(s._h, 0)
+        assert n == 6 * 2 * 3 * (cfg.nx + 16) * (cfg.nx + 6)      # zones x {p, v_r} x 3 planes x padded plane
+        assert s.lib.solar_gpu_planes_size(s._h, 5) == 6 * 5 * 5 * (cfg.nx + 16) * (cfg.nx + 6)
+        buf = torch.zeros(n, dtype=torch.float64, device="cuda")
+        p = ctypes.c_void_p(buf.data_ptr())
+        assert s.lib.solar_gpu_pack_planes(s._h, 0, 0, p) == _lib.SOLAR_ERR_ARG     # no slab below plane 0
+        _lib.check(s.lib.solar_gpu_pack_planes(s._h, 0, 1, p))
+
+
 def test_step_phases_equal_rk4(cfg):
     q0 = initial_state(cfg)
     with Solver(cfg) as a, Solver(cfg) as b:
@@ -95,7 +203,7 @@ def test_step_phases_equal_rk4(cfg):
         b.set_state(q0)
         a.rk4(2)
         for _ in range(2):
-            for phase in range(6):
+            for phase in (0, 1, 2, 3, 4, 6, 7):             # the filter phase in its two halves
                 _lib.check(b.lib.solar_gpu_step_phase(b._h, phase))
         b.synchronize()
         np.testing.assert_array_equal(a.get_state(), b.get_state())
@@ -136,7 +244,7 @@ def test_line_pack_roundtrip_and_errors(cfg):
         assert not back[~mask].any()
         bad = (ctypes.c_int * 2)(6, 0)
         assert s.lib.solar_gpu_pack_lines(s._h, 0, bad, 1, ctypes.c_void_p(buf.data_ptr())) == _lib.SOLAR_ERR_ARG
-        assert s.lib.solar_gpu_step_phase(s._h, 6) == _lib.SOLAR_ERR_ARG
+        assert s.lib.solar_gpu_step_phase(s._h, 8) == _lib.SOLAR_ERR_ARG
         assert s.lib.solar_gpu_set_owned_zones(s._h, 4, 3) == _lib.SOLAR_ERR_ARG
 
 

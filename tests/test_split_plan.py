@@ -140,3 +140,118 @@ def test_line_exchange_over_gloo(world):
         p.join(timeout=60)
         assert p.exitcode == 0
     assert res == {r: 0 for r in range(world)}
+
+
+# ---------------------------------------------------------------- zones x radial slabs
+def test_layout_and_slabs():
+    assert [D.layout(w) for w in (1, 2, 3, 4, 6, 8, 12)] == [(1, 1), (2, 1), (3, 1), (2, 2), (6, 1), (2, 4), (6, 2)]
+    assert D.layout(5) == (1, 5)
+    assert D.slabs(128, 4) == [(0, 32), (32, 64), (64, 96), (96, 128)]
+    assert D.slabs(20, 4) == [(0, 5), (5, 10), (10, 15), (15, 20)]
+    with pytest.raises(ValueError):
+        D.slabs(16, 4)                       # 4 planes per slab: the 5-plane filter halo would span two
+
+
+@pytest.mark.parametrize("world", [4, 8])
+def test_slab_plans_of_neighbours_agree(routes, world):
+    ngroups, nsl = D.layout(world)
+    plans = [D.slab_plan(world, r) for r in range(world)]
+    for r in range(world):
+        (sends, recvs), below, above = plans[r]
+        zg, sl = divmod(r, nsl)
+        for peer, pairs in sends.items():
+            assert peer % nsl == sl                              # zone lines stay inside the slab
+            assert plans[peer][0][1][r] == pairs
+        assert (below is None) == (sl == 0) and (above is None) == (sl == nsl - 1)
+        if below is not None:
+            assert plans[below][2] == r                          # I am my lower neighbour's upper one
+        if above is not None:
+            assert plans[above][1] == r
+
+
+class _FakePlanePacker:
+    """Boundary planes of one rank, coded by (rank, side, phase); received codes are kept."""
+
+    def __init__(self, rank):
+        self.rank = rank
+        self.got = {}
+
+    def size(self, phase):
+        return 7 if phase < 5 else 12         # stages share one size, the filter another
+
+    def pack(self, phase, side, buf):
+        import torch
+        buf.copy_(torch.full((self.size(phase),), float(self.rank * 100 + side * 10 + phase), dtype=torch.float64))
+
+    def unpack(self, phase, side, buf):
+        self.got[(phase, side)] = buf.numpy().copy()
+
+
+def _slab_rank_main(rank, world, port, out):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        ngroups, nsl = D.layout(world)
+        zg, sl = divmod(rank, nsl)
+        plan, below, above = D.slab_plan(world, rank)
+        own = D.owners(D.partition(ngroups))
+        own_rank = [D.rank_of(g, sl, nsl) for g in own]          # owner of each zone in my slab
+        lines = _FakePacker(own_rank, rank)
+        planes = _FakePlanePacker(rank)
+        alloc = lambda n: torch.zeros(n, dtype=torch.float64)
+        lx = D.LineExchange(plan, lines, D.p2p_transport(None), alloc)
+        px = D.PlaneExchange(below, above, planes, D.p2p_transport(None), alloc)
+        phases = []
+
+        def step(phase):                     # the kernels of a phase (nothing to move here)
+            phases.append(phase)
+        bad = 0
+        routes = D.route_table()
+        for phase in range(5):
+            lines.fill(phase)
+            lx.run(phase)
+            px.run(phase)
+            step(phase)
+            for z in range(6):
+                if own_rank[z] != rank:
+                    continue
+                for e in range(4):
+                    pair = (int(routes[z, e, 0]), int(routes[z, e, 1]))
+                    if not np.array_equal(lines.store[pair], _code(pair, phase, 3)):
+                        bad += 1
+        lines.fill(5)
+        lx.run(5)
+        step(6)
+        px.run(5)
+        step(7)
+        if phases != [0, 1, 2, 3, 4, 6, 7]:
+            bad += 1
+        for phase in (0, 1, 2, 3, 4, 5):
+            for side, peer in ((0, below), (1, above)):
+                if peer is None:
+                    continue
+                want = float(peer * 100 + (1 - side) * 10 + phase)      # the peer's send toward me
+                if not np.all(planes.got[(phase, side)] == want):
+                    bad += 1
+        out.put((rank, bad))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [4, 8])
+def test_zone_and_slab_exchange_over_gloo(world):
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_slab_rank_main, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=180) for _ in range(world))
+    for p in procs:
+        p.join(timeout=60)
+    assert res == {r: 0 for r in range(world)}
