@@ -322,7 +322,8 @@ def e2e_block(cfg, precision: str, nfields: int, args, world: int, local: int):
     import torch
     from solar_b200.solver import Solver
 
-    state_bytes = 6 * 5 * cfg.nr * cfg.nx * cfg.nx * 8
+    # the stored fields cross PCIe as FP64 (rho is not stored with 4 fields: not copied)
+    state_bytes = 6 * nfields * cfg.nr * cfg.nx * cfg.nx * 8
     host = torch.empty(6 * 5 * cfg.nr * cfg.nx * cfg.nx, dtype=torch.float64, pin_memory=True).numpy()
     out = torch.empty_like(torch.from_numpy(host)).pin_memory().numpy()
     norms = torch.empty(args.steps, dtype=torch.float64, pin_memory=True).numpy()
@@ -341,9 +342,9 @@ def e2e_block(cfg, precision: str, nfields: int, args, world: int, local: int):
             "h2d_bytes_per_step": state_bytes / args.steps,
             "d2h_bytes_per_step": (state_bytes + 8 * args.steps) / args.steps,
             "ms_per_step": te * 1e3 / args.steps, "norm_vr_last": float(norms[-1]),
-            "note": "state in from pinned host memory once per job, K RK4 steps each followed by "
-                    "norm(v_r) (cube.f90:74-78) kept on the device and read back once, state out at "
-                    "the end; host wall clock of the whole job"}
+            "note": "state in from pinned host memory once per job (the stored fields, FP64), K RK4 "
+                    "steps each followed by norm(v_r) (cube.f90:74-78) kept on the device and read "
+                    "back once, state out at the end; host wall clock of the whole job"}
 
 
 def batch_block(device: int):

@@ -161,6 +161,29 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const __grid_cons
   for (int q = 0; q < 7; ++q) { w1[q] = T(0); w2[q] = T(0); }
 #pragma unroll
   for (int q = 0; q < 4; ++q) { pp[q] = T(0); pv[q] = T(0); }
+  // The 2-D metric terms of the own point and of the halo point are the same on every plane:
+  // in float they are held in registers for the whole chunk (the per-plane reads were the
+  // kernel's main long-scoreboard stall); in double the 128-register budget has no room and
+  // they are read per plane.
+  constexpr bool HOLD = sizeof(T) == 4;
+  T gD = T(0), gXYD = T(0), gC = T(0), gXYC = T(0), gDivX = T(0), gDivY = T(0), gTX = T(0), gTY = T(0);
+  T gh1 = T(0), gh2 = T(0), gh3 = T(0);
+  if (HOLD) {
+    gD = __ldg(met + mD * P2 + p2);
+    gXYD = __ldg(met + mXYD * P2 + p2);
+    gC = __ldg(met + mC * P2 + p2);
+    gXYC = __ldg(met + mXYC * P2 + p2);
+    gDivX = __ldg(met + mDivX * P2 + p2);
+    gDivY = __ldg(met + mDivY * P2 + p2);
+    gTX = __ldg(met + mTX * P2 + p2);
+    gTY = __ldg(met + mTY * P2 + p2);
+    if (h_in) {
+      gh1 = __ldg(met + (xi_halo ? mD : mXYD) * P2 + hq2);
+      gh2 = __ldg(met + (xi_halo ? mXYC : mC) * P2 + hq2);
+      gh3 = __ldg(met + (xi_halo ? mDivX : mDivY) * P2 + hq2);
+    }
+  }
+  auto metric = [&](int row, T held) { return HOLD ? held : __ldg(met + row * P2 + p2); };
   int slot = 0;
   uint32_t phase = 0;
   bool ok = true, failed = false;
@@ -218,12 +241,12 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const __grid_cons
       r1 = -inv_rho0 * mp[kVr];
       r2 = e;
       if (own) {
-        const T tD = __ldg(met + mD * P2 + p2), tXYD = __ldg(met + mXYD * P2 + p2), tC = __ldg(met + mC * P2 + p2);
-        const T tXYC = __ldg(met + mXYC * P2 + p2);
+        const T tD = metric(mD, gD), tXYD = metric(mXYD, gXYD), tC = metric(mC, gC);
+        const T tXYC = metric(mXYC, gXYC);
         sX1[ty][tx + 3] = -invr * inv_rho0 * (tD * mp[kVxi] + tXYC * mp[kVeta]);
-        sX2[ty][tx + 3] = invr * __ldg(met + mDivX * P2 + p2) * e;
+        sX2[ty][tx + 3] = invr * metric(mDivX, gDivX) * e;
         sY1[ty + 3][tx] = -invr * inv_rho0 * (tXYD * mp[kVxi] + tC * mp[kVeta]);
-        sY2[ty + 3][tx] = invr * __ldg(met + mDivY * P2 + p2) * e;
+        sY2[ty + 3][tx] = invr * metric(mDivY, gDivY) * e;
         if (has_halo) {
           T v1 = T(0), v2 = T(0);
           if (do_halo) {
@@ -233,9 +256,9 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const __grid_cons
             const T hp = sb[5 * PBs + hb] + a.beta * sb[4 * PBs + hb];
             const T hr = has_rho ? sb[7 * PBs + hb] + a.beta * sb[6 * PBs + hb] : T(0);
             const T he = -(a.c2 ? hc2 * rho0 : c2r) * hp - rho0 * hr;
-            const T hm1 = __ldg(met + (xi_halo ? mD : mXYD) * P2 + hq2);
-            const T hm2 = __ldg(met + (xi_halo ? mXYC : mC) * P2 + hq2);
-            const T hm3 = __ldg(met + (xi_halo ? mDivX : mDivY) * P2 + hq2);
+            const T hm1 = HOLD ? gh1 : __ldg(met + (xi_halo ? mD : mXYD) * P2 + hq2);
+            const T hm2 = HOLD ? gh2 : __ldg(met + (xi_halo ? mXYC : mC) * P2 + hq2);
+            const T hm3 = HOLD ? gh3 : __ldg(met + (xi_halo ? mDivX : mDivY) * P2 + hq2);
             v1 = -invr * inv_rho0 * (hm1 * hx + hm2 * hy);
             v2 = invr * hm3 * he;
           }
@@ -246,8 +269,8 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const __grid_cons
         const T sig = __ldg(rad + rSigma * nr + m);
         T pw[5];
         pw[kRho] = -__ldg(rad + rG0Rho0 * nr + m) * mp[kVr] - sig * mu[kRho];
-        pw[kVxi] = -invr * __ldg(met + mTX * P2 + p2) * e;
-        pw[kVeta] = -invr * __ldg(met + mTY * P2 + p2) * e;
+        pw[kVxi] = -invr * metric(mTX, gTX) * e;
+        pw[kVeta] = -invr * metric(mTY, gTY) * e;
         pw[kVr] = T(2) * invr * e - __ldg(rad + rDRho0 * nr + m) * mp[kRho] + __ldg(rad + rRho0G0 * nr + m) * mp[kP] -
                   sig * mu[kVr];
         pw[kP] = -sig * mu[kP];

@@ -595,16 +595,15 @@ static int download_fields(solar_ctx* c, const void* buf, int run, double* host,
     for (int m = 0; m < nfields_h; ++m) {
       const int f = fields[m];
       const int s = c->g.slot[f];
-      if (c->fp32) {
-        const float* src = s < 0 ? nullptr : (const float*)buf + c->g.vol(run, z, s);
-        pack_kernel<float><<<blocks, threads, 0, c->stream>>>(src, c->stage64, c->g);
-      } else {
-        const double* src = s < 0 ? nullptr : (const double*)buf + c->g.vol(run, z, s);
-        pack_kernel<double><<<blocks, threads, 0, c->stream>>>(src, c->stage64, c->g);
+      double* dst = host + ((long long)z * nh + m) * V;
+      if (s < 0) {                     // a field the context does not store reads back as zero
+        std::memset(dst, 0, (size_t)V * sizeof(double));
+        continue;
       }
+      if (c->fp32) pack_kernel<float><<<blocks, threads, 0, c->stream>>>((const float*)buf + c->g.vol(run, z, s), c->stage64, c->g);
+      else pack_kernel<double><<<blocks, threads, 0, c->stream>>>((const double*)buf + c->g.vol(run, z, s), c->stage64, c->g);
       CK(cudaGetLastError());
-      CK(cudaMemcpyAsync(host + ((long long)z * nh + m) * V, c->stage64, V * sizeof(double),
-                         cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaMemcpyAsync(dst, c->stage64, V * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     }
   CK(cudaStreamSynchronize(c->stream));
   return SOLAR_OK;
