@@ -44,6 +44,7 @@ template <typename T>
 struct AdjStageArgs {
   CUtensorMap mBq, mBw;   // boxes (TX+8) x (TY+6) of lq / lw
   CUtensorMap mTq, mTw;   // tiles TX x TY of lq / lw
+  CUtensorMap mC2, mDiv;  // tiles TX x TY of the compact c^2 / stored divergence (when present)
   T* lout;
   T* lwout;
   T* rb;              // [face][4][2][n*n] raw R1, R2 of planes 1, 2, nr-3, nr-2
@@ -66,8 +67,10 @@ struct AdjLayout {
   static constexpr size_t P_BYTES = align128(PB * sizeof(T));
   static constexpr size_t O_BYTES = align128(OB * sizeof(T));
   // a chunk plane: boxes [v_xi, v_eta, p, rho] x [lq, lw], then the v_r tiles [lq, lw];
-  // an extra plane: tiles [p, rho, v_r] x [lq, lw] from the slot's start
-  static constexpr size_t SLOT = 8 * P_BYTES + 2 * O_BYTES;
+  // an extra plane: tiles [p, rho, v_r] x [lq, lw] from the slot's start; every plane: the
+  // c^2 tile and (chunk planes) the stored-divergence tile after them
+  static constexpr size_t AUX = 8 * P_BYTES + 2 * O_BYTES;
+  static constexpr size_t SLOT = AUX + 2 * O_BYTES;
   static constexpr int RING = AdjRing<T>::value;
   static constexpr size_t BAR = RING * SLOT;
   static constexpr size_t TOTAL = BAR + RING * sizeof(uint64_t);
@@ -119,12 +122,18 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const __grid_cons
   const int zf = face * g.nf;            // plane index of (slot s, k) = (zf + s) * nr + k (run 0)
   const int xB = IOFF + i0 - 4, yB = JOFF + j0 - 3, xT = IOFF + i0, yT = JOFF + j0;
   auto slot_base = [&](int sl) { return smem + (size_t)sl * L::SLOT; };
+  const bool tc2 = a.c2 != nullptr, tdiv = a.grad != nullptr;   // c^2 / divergence tiles in the ring
+  const int zc = face * nr;                // plane index of the compact arrays: face * nr + k
   auto issue = [&](int m, int sl) {
     uint64_t* bar = &bars[sl];
     unsigned char* base = slot_base(sl);
-    if (m >= kb && m < ke) {
+    const bool chunk = m >= kb && m < ke;
+    if (tc2) tma_load_3d(base + L::AUX, &a.mC2, i0, j0, zc + m, bar);
+    if (tdiv && chunk) tma_load_3d(base + L::AUX + L::O_BYTES, &a.mDiv, i0, j0, zc + m, bar);
+    const uint32_t aux = (uint32_t)(((tc2 ? 1 : 0) + (tdiv && chunk ? 1 : 0)) * L::OB * sizeof(T));
+    if (chunk) {
       const int nbox = has_rho ? 4 : 3;
-      mbar_expect_tx(bar, (uint32_t)((2 * nbox * L::PB + 2 * L::OB) * sizeof(T)));
+      mbar_expect_tx(bar, (uint32_t)((2 * nbox * L::PB + 2 * L::OB) * sizeof(T)) + aux);
       const int bs[4] = {sX, sY, sP, sRho};
       for (int f = 0; f < nbox; ++f) {
         tma_load_3d(base + (2 * f) * L::P_BYTES, &a.mBq, xB, yB, (zf + bs[f]) * nr + m, bar);
@@ -134,7 +143,7 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const __grid_cons
       tma_load_3d(base + 8 * L::P_BYTES + L::O_BYTES, &a.mTw, xT, yT, (zf + sR) * nr + m, bar);
     } else {
       const int nt = has_rho ? 3 : 2;
-      mbar_expect_tx(bar, (uint32_t)(2 * nt * L::OB * sizeof(T)));
+      mbar_expect_tx(bar, (uint32_t)(2 * nt * L::OB * sizeof(T)) + aux);
       const int ts[3] = {sP, sR, sRho};
       for (int f = 0; f < nt; ++f) {
         tma_load_3d(base + (2 * f) * L::O_BYTES, &a.mTq, xT, yT, (zf + ts[f]) * nr + m, bar);
@@ -197,9 +206,7 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const __grid_cons
     if (real) {
       const int o = m * plane + own0;
       const long long plane_c2 = (long long)(face_c2 + m) * P2;
-      // global loads that do not come through the ring
-      const T c2own = a.c2 ? __ldg(a.c2 + plane_c2 + p2) : T(0);
-      const T divv = (own && a.grad) ? __ldg(a.div + plane_c2 + p2) : T(0);
+      // the halo point's c^2 does not come through the ring
       const bool do_halo = own && h_in && !bc;
       const T hc2 = (do_halo && a.c2) ? __ldg(a.c2 + plane_c2 + hq2) : T(0);
       const T invr = __ldg(rad + rInvR * nr + m), inv_rho0 = __ldg(rad + rInvRho0 * nr + m);
@@ -210,6 +217,9 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const __grid_cons
       }
       const T* sb = reinterpret_cast<const T*>(slot_base(slot));
       constexpr int PBs = (int)(L::P_BYTES / sizeof(T)), OBs = (int)(L::O_BYTES / sizeof(T));
+      const T* saux = reinterpret_cast<const T*>(slot_base(slot) + L::AUX);
+      const T c2own = tc2 ? saux[to] : T(0);
+      const T divv = (own && tdiv) ? saux[OBs + to] : T(0);
       T lqv[5], lwv[5];
 #pragma unroll
       for (int f = 0; f < 5; ++f) { lqv[f] = T(0); lwv[f] = T(0); }

@@ -97,8 +97,11 @@ static int launch_adj_stage(solar_ctx* c, AdjStageArgs<T>& a) {
   using L = AdjLayout<T, TX, TY>;
   AdjBuffers& b = c->adj;
   if (!make_map(c, b.L, TX + 8, TY + 6, &a.mBq) || !make_map(c, b.LW, TX + 8, TY + 6, &a.mBw) ||
-      !make_map(c, b.L, TX, TY, &a.mTq) || !make_map(c, b.LW, TX, TY, &a.mTw))
+      !make_map(c, b.L, TX, TY, &a.mTq) || !make_map(c, b.LW, TX, TY, &a.mTw) ||
+      (a.c2 && !make_compact_map(c, a.c2, TX, TY, &a.mC2)) || (a.grad && !make_compact_map(c, a.div, TX, TY, &a.mDiv)))
     return fail(SOLAR_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+  if (!a.c2) a.mC2 = a.mTq;                       // unused
+  if (!a.grad) a.mDiv = a.mTq;
   static bool attr_set = false;
   if (!attr_set) {
     CK(cudaFuncSetAttribute(adj_stage_kernel<T, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::TOTAL));

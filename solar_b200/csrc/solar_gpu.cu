@@ -248,6 +248,22 @@ static bool make_map(const solar_ctx* c, const void* base, int bx, int by, CUten
   return r == CUDA_SUCCESS;
 }
 
+// A compact six-zone field [face][k][j][i] (c^2, stored divergences) as a 3-D array:
+// x = i, y = j, z = face * nr + k; box bx x by x 1.
+static bool make_compact_map(const solar_ctx* c, const void* base, int bx, int by, CUtensorMap* m) {
+  auto enc = tensor_map_encoder();
+  if (!enc) return false;
+  const Geom& g = c->g;
+  cuuint64_t dims[3] = {(cuuint64_t)g.n, (cuuint64_t)g.n, (cuuint64_t)6 * g.nr};
+  cuuint64_t strides[2] = {(cuuint64_t)g.n * c->esize, (cuuint64_t)g.n * g.n * c->esize};
+  cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = enc(m, c->fp32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
+                   const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
 // Staging windows of the edge kernel: the receiving edge is cut into segments of ts
 // positions (one thread per layer and position); a segment's ghost points read the source
 // positions [min s0t, max s0t + 9), widened to whole 16-byte pieces.
