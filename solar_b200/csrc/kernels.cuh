@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 
+#include "scheme.h"
 #include "tma.cuh"
 
 namespace solar {
@@ -798,16 +799,25 @@ struct FilterLayout {
   static constexpr size_t TOTAL = BAR + kFiltRing * sizeof(uint64_t);
 };
 
-// Each thread owns V consecutive points of one row (V = 16 bytes / sizeof(T)); the CTA
-// has (TX/V) x TY threads.  Per plane: the xi filter of every row of the box (rows
-// outside the face keep the unfiltered halo) goes to shared memory with 16-byte loads
-// and stores, then each thread eta-filters its V points and pushes them into an 11-deep
-// register queue; the k loop is unrolled by 11 so the queue indices are constants.
-template <typename T, int TX, int TY>
-__global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) filter_kernel(const __grid_constant__ FilterArgs<T> a) {
+// Each thread owns V consecutive points (V = 16 bytes / sizeof(T)) in each of R consecutive
+// rows; the CTA has (TX/V) x (TY/R) threads.  Per plane: every thread xi-filters its own R
+// rows of the box (rows outside the face keep the unfiltered halo), keeps them in registers
+// and stores them to shared memory with 16-byte stores, and the first thread rows also
+// filter the 6 halo rows of the box.  After one barrier each thread reads the 3 xi-filtered
+// rows above and the 3 below its own, eta-filters its R x V points and pushes them into an
+// 11-deep register queue; the k loop is unrolled by 11 so the queue indices are constants.
+// With R = 2 a thread reads 6 rows from shared memory for 2 output rows instead of 7 for 1.
+// The float kernel's bound of four CTAs per SM lets the compiler use 91 registers: at 6 x
+// 128^3 it ran in 100 us against 106 us at 88 registers (a bound of five) and 115 us at 83
+// (no bound).  The filter weights are compile-time values (scheme.h).
+template <typename T, int TX, int TY, int R>
+__global__ void __launch_bounds__((TX / Vec16<T>::V) * (TY / R), sizeof(T) == 4 ? 4 : 1) filter_kernel(const __grid_constant__ FilterArgs<T> a) {
   constexpr int V = Vec16<T>::V;
   constexpr int NT = TX / V;                 // threads per row
+  constexpr int NY = TY / R;                 // thread rows
   constexpr int NV = (V + 8) / V;            // vectors covering columns c-4 .. c+V+3
+  constexpr int NP = V / 2;                  // float pairs per row (float only)
+  static_assert(TY % R == 0, "the rows per thread divide the tile height");
   using L = FilterLayout<T, TX, TY>;
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L::BAR);
@@ -830,6 +840,7 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) filter_kernel(const _
   const int rz = rest / g.nf;
   const int run = a.runs ? a.runs[rz / g.nface] : rz / g.nface, face = g.face0 + rz % g.nface;
   const int cx = threadIdx.x, ty = threadIdx.y, tid = ty * NT + cx;
+  const int rb = R * ty;                     // first own row of the tile
   constexpr int PW = TX + 8;
   const int z0 = ((run * 6 + face) * g.nf + s) * nr;
   const int xP = IOFF + i0 - 4, yP = JOFF + j0 - 3;
@@ -849,19 +860,41 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) filter_kernel(const _
   const bool loads = !a.wc.no_loads;
   if (tid == 0 && loads)
     for (int k = ks; k < min(ks + kFiltRing, ke); ++k) issue(k, k - ks);
-  T* out = a.qout + g.vol(run, face, s) + g.at(0, j0 + ty, i0 + V * cx);
-  const T f0 = Coef<T>::filt(0), f1 = Coef<T>::filt(1), f2 = Coef<T>::filt(2), f3 = Coef<T>::filt(3);
-  // radial queue of eta-filtered planes; in float the four values of a thread are held as
-  // two packed pairs and the eta and radial filters run on pairs
+  T* out = a.qout + g.vol(run, face, s) + g.at(0, j0 + rb, i0 + V * cx);
+  constexpr T f0 = T(kFilt[0]), f1 = T(kFilt[1]), f2 = T(kFilt[2]), f3 = T(kFilt[3]);
+  constexpr T rw[6] = {T(kFiltR[0]), T(kFiltR[1]), T(kFiltR[2]), T(kFiltR[3]), T(kFiltR[4]), T(kFiltR[5])};
+  // xi filter of box row r (tile row r - 3) at columns V*cx .. V*cx+V-1 of the tile
+  auto xi_row = [&](const T* bx, int r, T* v) {
+    const int jr = j0 - 3 + r;
+    T w[NV * V];
+#pragma unroll
+    for (int m = 0; m < NV; ++m) ldv(bx + r * PW + V * cx + m * V, w + m * V);
+    // w[q'] holds box column V*cx + q'; the own point q sits at box column V*cx + 4 + q
+    constexpr int o = 4;
+    if (jr < 0 || jr >= n) {
+#pragma unroll
+      for (int q = 0; q < V; ++q) v[q] = w[o + q];
+    } else {
+#pragma unroll
+      for (int q = 0; q < V; ++q)
+        v[q] = f0 * w[o + q] + f1 * (w[o + q - 1] + w[o + q + 1]) + f2 * (w[o + q - 2] + w[o + q + 2]) +
+               f3 * (w[o + q - 3] + w[o + q + 3]);
+    }
+  };
+  // radial queue of eta-filtered planes; in float the V values of a thread's row are held
+  // as packed pairs and the eta and radial filters run on pairs
   constexpr bool PAIRS = sizeof(T) == 4;
-  T tq[11][V];
-  unsigned long long tq2[11][2];
+  T tq[11][R][V];
+  unsigned long long tq2[11][R][NP > 0 ? NP : 1];
 #pragma unroll
-  for (int m = 0; m < 11; ++m) {
+  for (int m = 0; m < 11; ++m)
 #pragma unroll
-    for (int q = 0; q < V; ++q) tq[m][q] = T(0);
-    tq2[m][0] = tq2[m][1] = 0ull;
-  }
+    for (int r = 0; r < R; ++r) {
+#pragma unroll
+      for (int q = 0; q < V; ++q) tq[m][r][q] = T(0);
+#pragma unroll
+      for (int h = 0; h < (NP > 0 ? NP : 1); ++h) tq2[m][r][h] = 0ull;
+    }
   T zero[V];
 #pragma unroll
   for (int q = 0; q < V; ++q) zero[q] = T(0);
@@ -880,83 +913,86 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) filter_kernel(const _
       const bool got = mbar_wait(&bars[slot], phase, a.wc, kErrFilterRing);
       const T* bx = reinterpret_cast<const T*>(smem + slot * L::P_BYTES);
       T* t1 = reinterpret_cast<T*>(smem + kFiltRing * L::P_BYTES + (k & 1) * L::S_BYTES);
-      // xi filter of the box rows (columns V*cx .. V*cx+V-1 of the tile)
-      for (int r = ty; r < TY + 6; r += TY) {
-        const int jr = j0 - 3 + r;
-        T w[NV * V];
+      // c[m] holds xi-filtered box row rb + m (tile row rb - 3 + m)
+      T c[R + 6][V];
 #pragma unroll
-        for (int m = 0; m < NV; ++m) ldv(bx + r * PW + V * cx + m * V, w + m * V);
-        // w[q'] holds box column V*cx + q'; the own point q sits at box column V*cx + 4 + q
-        constexpr int o = 4;
+      for (int r = 0; r < R; ++r) {
+        xi_row(bx, rb + 3 + r, c[3 + r]);
+        stv(t1 + (rb + 3 + r) * TX + V * cx, c[3 + r]);
+      }
+      // the halo rows of the box: 0..2 and TY+3..TY+5
+      for (int h = ty; h < 6; h += NY) {
+        const int r = h < 3 ? h : TY + h;
         T v[V];
-        if (jr < 0 || jr >= n) {
-#pragma unroll
-          for (int q = 0; q < V; ++q) v[q] = w[o + q];
-        } else {
-#pragma unroll
-          for (int q = 0; q < V; ++q)
-            v[q] = f0 * w[o + q] + f1 * (w[o + q - 1] + w[o + q + 1]) + f2 * (w[o + q - 2] + w[o + q + 2]) +
-                   f3 * (w[o + q - 3] + w[o + q + 3]);
-        }
+        xi_row(bx, r, v);
         stv(t1 + r * TX + V * cx, v);
       }
       if (__syncthreads_or(!got)) { ok = false; fail_at = 2 * k + (got ? 1 : 0); break; }
       if (tid == 0 && loads && k + kFiltRing < ke) issue(k + kFiltRing, slot);
       if (++slot == kFiltRing) { slot = 0; phase ^= 1; }
-      // eta filter of this thread's V points (rows ty .. ty+6 of the xi-filtered tile)
-      T c[7][V];
 #pragma unroll
-      for (int m = 0; m < 7; ++m) ldv(t1 + (ty + m) * TX + V * cx, c[m]);
-      if constexpr (PAIRS) {
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const float* cf = reinterpret_cast<const float*>(&c[0][0]);
-          auto pr = [&](int m) { return pk2(cf[m * V + 2 * h], cf[m * V + 2 * h + 1]); };
-          unsigned long long t = mul2(pk2(f0, f0), pr(3));
-          t = fma2(pk2(f1, f1), add2(pr(2), pr(4)), t);
-          t = fma2(pk2(f2, f2), add2(pr(1), pr(5)), t);
-          tq2[u][h] = fma2(pk2(f3, f3), add2(pr(0), pr(6)), t);
-        }
-      } else {
-#pragma unroll
-        for (int q = 0; q < V; ++q)
-          tq[u][q] = f0 * c[3][q] + f1 * (c[2][q] + c[4][q]) + f2 * (c[1][q] + c[5][q]) + f3 * (c[0][q] + c[6][q]);
+      for (int m = 0; m < 3; ++m) {
+        ldv(t1 + (rb + m) * TX + V * cx, c[m]);
+        ldv(t1 + (rb + R + 3 + m) * TX + V * cx, c[R + 3 + m]);
       }
-      if (k - ks >= 10) {
-        // planes k-10 .. k sit at queue rows (u+1 .. u+11) % 11; the centre is k-5
-        T v[V];
+      // eta filter of own row r: rows r .. r+6 of c
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
         if constexpr (PAIRS) {
 #pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const float r0 = Coef<float>::filtr(0);
-            unsigned long long acc = mul2(pk2(r0, r0), tq2[(u + 6) % 11][h]);
-#pragma unroll
-            for (int m = 1; m <= 5; ++m) {
-              const float rm = Coef<float>::filtr(m);
-              acc = fma2(pk2(rm, rm), add2(tq2[(u + 6 - m) % 11][h], tq2[(u + 6 + m) % 11][h]), acc);
-            }
-            float x, y;
-            upk2(acc, x, y);
-            v[2 * h] = x;
-            v[2 * h + 1] = y;
+          for (int h = 0; h < NP; ++h) {
+            auto pr = [&](int m) { return pk2(c[r + m][2 * h], c[r + m][2 * h + 1]); };
+            unsigned long long t = mul2(pk2(f0, f0), pr(3));
+            t = fma2(pk2(f1, f1), add2(pr(2), pr(4)), t);
+            t = fma2(pk2(f2, f2), add2(pr(1), pr(5)), t);
+            tq2[u][r][h] = fma2(pk2(f3, f3), add2(pr(0), pr(6)), t);
           }
         } else {
 #pragma unroll
-          for (int q = 0; q < V; ++q) {
-            T acc = Coef<T>::filtr(0) * tq[(u + 6) % 11][q];
-#pragma unroll
-            for (int m = 1; m <= 5; ++m) acc += Coef<T>::filtr(m) * (tq[(u + 6 - m) % 11][q] + tq[(u + 6 + m) % 11][q]);
-            v[q] = acc;
-          }
+          for (int q = 0; q < V; ++q)
+            tq[u][r][q] = f0 * c[r + 3][q] + f1 * (c[r + 2][q] + c[r + 4][q]) + f2 * (c[r + 1][q] + c[r + 5][q]) +
+                          f3 * (c[r][q] + c[r + 6][q]);
         }
-        stv(out + (long long)(k - 5) * g.plane, v);
+      }
+      if (k - ks >= 10) {
+        // planes k-10 .. k sit at queue rows (u+1 .. u+11) % 11; the centre is k-5
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          T v[V];
+          if constexpr (PAIRS) {
+#pragma unroll
+            for (int h = 0; h < NP; ++h) {
+              unsigned long long acc = mul2(pk2(rw[0], rw[0]), tq2[(u + 6) % 11][r][h]);
+#pragma unroll
+              for (int m = 1; m <= 5; ++m) {
+                acc = fma2(pk2(rw[m], rw[m]), add2(tq2[(u + 6 - m) % 11][r][h], tq2[(u + 6 + m) % 11][r][h]), acc);
+              }
+              float x, y;
+              upk2(acc, x, y);
+              v[2 * h] = x;
+              v[2 * h + 1] = y;
+            }
+          } else {
+#pragma unroll
+            for (int q = 0; q < V; ++q) {
+              T acc = rw[0] * tq[(u + 6) % 11][r][q];
+#pragma unroll
+              for (int m = 1; m <= 5; ++m)
+                acc += rw[m] * (tq[(u + 6 - m) % 11][r][q] + tq[(u + 6 + m) % 11][r][q]);
+              v[q] = acc;
+            }
+          }
+          stv(out + (long long)(k - 5) * g.plane + r * g.pitch, v);
+        }
       }
     }
   }
   // the five end planes at each radial end are zero (filter.f90:726-775)
   for (int m = 0; m < 10; ++m) {
     const int k = m < 5 ? m : nr - 10 + m;
-    if (k >= ko0 && k < ko1) stv(out + (long long)k * g.plane, zero);
+    if (k >= ko0 && k < ko1)
+#pragma unroll
+      for (int r = 0; r < R; ++r) stv(out + (long long)k * g.plane + r * g.pitch, zero);
   }
   if (!ok && tid == 0 && loads) {
     // at the break on plane k, planes [ks, min(k + kFiltRing, ke)) were issued

@@ -416,7 +416,7 @@ static int launch_stage(solar_ctx* c, const void* qin, void* qout, int mode, int
   return fail(SOLAR_ERR_ARG, "unsupported stage tile %d x %d", tx, ty);
 }
 
-template <typename T, int TX, int TY>
+template <typename T, int TX, int TY, int R>
 static int launch_filter_t(solar_ctx* c, const void* qin, void* qout, const int* runs) {
   using L = FilterLayout<T, TX, TY>;
   FilterArgs<T> a;
@@ -427,36 +427,51 @@ static int launch_filter_t(solar_ctx* c, const void* qin, void* qout, const int*
   a.g = c->g;
   static bool attr_set = false;
   static int resident = 1;
-  const int threads = (TX / Vec16<T>::V) * TY;
+  const int threads = (TX / Vec16<T>::V) * (TY / R);
   if (!attr_set) {
-    CK(cudaFuncSetAttribute(filter_kernel<T, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::TOTAL));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, filter_kernel<T, TX, TY>, threads, L::TOTAL));
+    CK(cudaFuncSetAttribute(filter_kernel<T, TX, TY, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::TOTAL));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, filter_kernel<T, TX, TY, R>, threads, L::TOTAL));
     resident = std::max(resident, 1);
     attr_set = true;
   }
   // Whole-column CTAs for every full wave; the units of a last, partial wave are cut into
-  // radial chunks (at least 11 planes each) so that they fill one wave.
+  // radial chunks (at least 11 planes each) so that they fill one wave.  When every unit
+  // fits in one wave, SMs would hold units / nsm or one more whole column: the units past
+  // an even share are cut into chunks, about one per SM, which run in the spare CTA slot
+  // beside the whole columns (6 x 128^3 float: 740 columns and 140 chunks of 118 / 5
+  // planes instead of 28 SMs with six columns).
   const long long units = (long long)(c->g.n / TX) * (c->g.n / TY) * c->g.nf * launched_runs(c, runs) * c->g.nface;
   const long long slots = (long long)c->nsm * resident;
-  const long long tail = units % slots;
+  const long long nk = c->g.k1 - c->g.k0;
   a.whole = (int)units;
   a.chunks = 1;
-  if (units > slots && tail > 0) {
-    const int chunks = (int)std::min<long long>((c->g.k1 - c->g.k0) / 11, std::max<long long>(1, (slots + tail / 2) / tail));
-    if (chunks > 1) {
-      a.whole = (int)(units - tail);
-      a.chunks = chunks;
-    }
+  long long cut = 0, chunks = 1;
+  if (units > slots) {
+    cut = units % slots;
+    if (cut > 0) chunks = std::min<long long>(nk / 11, std::max<long long>(1, (slots + cut / 2) / cut));
+  } else {
+    const long long per = units / c->nsm;
+    cut = units % c->nsm;
+    if (per >= 1 && per < resident && cut > 0) chunks = std::min<long long>(nk / 11, c->nsm / cut);
+  }
+  if (chunks > 1) {
+    a.whole = (int)(units - cut);
+    a.chunks = (int)chunks;
   }
   const long long grid = a.whole + (units - a.whole) * a.chunks;
-  CK(launch_pdl(filter_kernel<T, TX, TY>, dim3((unsigned)grid), dim3(TX / Vec16<T>::V, TY), L::TOTAL, c->stream, a));
+  CK(launch_pdl(filter_kernel<T, TX, TY, R>, dim3((unsigned)grid), dim3(TX / Vec16<T>::V, TY / R), L::TOTAL, c->stream, a));
   return SOLAR_OK;
 }
 
 template <typename T>
 static int launch_filter(solar_ctx* c, const void* qin, void* qout, const int* runs) {
-  if (c->g.n % 32 == 0) return launch_filter_t<T, 32, 16>(c, qin, qout, runs);
-  return launch_filter_t<T, 16, 16>(c, qin, qout, runs);
+  // Rows per thread: float keeps one row per thread (four warps of 91 registers, five CTAs
+  // to an SM); double takes two, which reads 6 rows of shared memory for 2 output rows
+  // (measured at 6 x 128^3: float 100 us with R = 1, 114-119 us with R = 2; double 250 us
+  // with R = 2, 282 us with R = 1).
+  constexpr int R = sizeof(T) == 4 ? 1 : 2;
+  if (c->g.n % 32 == 0) return launch_filter_t<T, 32, 16, R>(c, qin, qout, runs);
+  return launch_filter_t<T, 16, 16, R>(c, qin, qout, runs);
 }
 
 static int force_begin(solar_ctx* c);   // forcing.cuh: this step's source field

@@ -14,9 +14,6 @@ const double kBdy[3][7] = {
     {-2.192280339, 4.748611401, -5.108851915, 4.461567104, -2.833498741, 1.128328861, -0.203876371},
     {-0.209337622, -1.084875676, 2.147776050, -1.388928322, 0.768949766, -0.28181465, 0.048230454},
     {0.049041958, -0.468840357, -0.474760914, 1.273274737, -0.518484526, 0.166138533, -0.026369431}};
-// Symmetric filters: centre weight first; header:99-105 and header:123-133.
-const double kFilt[4] = {0.6875, 0.234375, -0.09375, 0.015625};
-const double kFiltR[6] = {0.753906, 0.2050775, -0.1171875, 0.043945, -0.0097655, 0.0009765};
 // header:68-76
 const double kAlpha[5] = {0.0, -4.801594388477952e-01, -1.404247195200064e+00,
                           -2.016477077503357e+00, -1.056444269767207e+00};

@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "../../include/solar_gpu.h"
+#include "scheme.h"
 
 namespace solar {
 
@@ -20,8 +21,8 @@ namespace solar {
 // (header:40-55, 68-76, 99-105, 123-133).
 extern const double kDrp[4];          // c0..c3 of the antisymmetric 7-point stencil
 extern const double kBdy[3][7];       // one-sided rows for the first three points
-extern const double kFilt[4];         // f0..f3 of the symmetric 7-point filter
-extern const double kFiltR[6];        // f0..f5 of the symmetric 11-point radial filter
+// kFilt (f0..f3 of the symmetric 7-point filter) and kFiltR (f0..f5 of the symmetric
+// 11-point radial filter) are in scheme.h.
 extern const double kAlpha[5];
 extern const double kBeta[5];
 
