@@ -31,7 +31,9 @@ namespace solar {
 // shared-memory slots, each guarded by an mbarrier: for a plane of the chunk, the lambda_q
 // and lambda_w boxes (tile plus a 4-column / 3-row halo) of v_xi, v_eta, p and rho and the
 // tiles of v_r; for the three extra planes on either side only the tiles of p, rho and v_r.
-// Per plane the kernel forms the coefficient-weighted volumes X1, X2 (on the tile and its
+// Every plane also brings its c^2 box (the halo points use it too), the stored divergence
+// tile (chunk planes) and its row of radial coefficients (an untiled bulk copy), so the
+// per-plane values need no global loads.  Per plane the kernel forms the coefficient-weighted volumes X1, X2 (on the tile and its
 // xi halo) and Y1, Y2 (tile and eta halo) in shared memory from mu = lw + beta lq (zero
 // outside the face and on the BC planes), applies -D_xi / -D_eta, and keeps facr * R1 and
 // facr * R2 of the last seven planes in registers for the banded part of the radial
@@ -44,7 +46,8 @@ template <typename T>
 struct AdjStageArgs {
   CUtensorMap mBq, mBw;   // boxes (TX+8) x (TY+6) of lq / lw
   CUtensorMap mTq, mTw;   // tiles TX x TY of lq / lw
-  CUtensorMap mC2, mDiv;  // tiles TX x TY of the compact c^2 / stored divergence (when present)
+  CUtensorMap mC2;        // boxes (TX+8) x (TY+6) of the compact c^2 (when present; zero outside the face)
+  CUtensorMap mDiv;       // tiles TX x TY of the compact stored divergence (when present)
   T* lout;
   T* lwout;
   T* rb;              // [face][4][2][n*n] raw R1, R2 of planes 1, 2, nr-3, nr-2
@@ -53,6 +56,8 @@ struct AdjStageArgs {
   double* grad;
   const T* rad;
   const T* met;
+  const T* radT;      // [nr][16]: the radial rows of a plane together (through the ring)
+  const T* met8;      // [n][n][8]: metric rows mD..mTY of a point together
   WaitCtl wc;         // error word and bound of the ring waits
   Geom g;
   T alpha, beta, dt, inv_dxi;
@@ -68,9 +73,12 @@ struct AdjLayout {
   static constexpr size_t O_BYTES = align128(OB * sizeof(T));
   // a chunk plane: boxes [v_xi, v_eta, p, rho] x [lq, lw], then the v_r tiles [lq, lw];
   // an extra plane: tiles [p, rho, v_r] x [lq, lw] from the slot's start; every plane: the
-  // c^2 tile and (chunk planes) the stored-divergence tile after them
+  // c^2 box (the halo points read it too) and (chunk planes) the stored-divergence tile
+  // after it, then the plane's row of radial coefficients (16 values, zero padded)
   static constexpr size_t AUX = 8 * P_BYTES + 2 * O_BYTES;
-  static constexpr size_t SLOT = AUX + 2 * O_BYTES;
+  static constexpr size_t DIV_OFF = AUX + P_BYTES;
+  static constexpr size_t RAD_OFF = DIV_OFF + O_BYTES;
+  static constexpr size_t SLOT = align128(RAD_OFF + 16 * sizeof(T));
   static constexpr int RING = AdjRing<T>::value;
   static constexpr size_t BAR = RING * SLOT;
   static constexpr size_t TOTAL = BAR + RING * sizeof(uint64_t);
@@ -99,7 +107,6 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const __grid_cons
   const int sRho = g.slot[kRho], sX = g.slot[kVxi], sY = g.slot[kVeta], sR = g.slot[kVr], sP = g.slot[kP];
   const bool has_rho = sRho >= 0;
   const T* __restrict__ met = a.met;
-  const T* __restrict__ rad = a.rad;
   const T c1 = Coef<T>::drp(1), c2c = Coef<T>::drp(2), c3 = Coef<T>::drp(3);
   // this thread's halo point: eta-halo rows first, then xi-halo columns
   const bool has_halo = tid < NHALO;
@@ -128,9 +135,10 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const __grid_cons
     uint64_t* bar = &bars[sl];
     unsigned char* base = slot_base(sl);
     const bool chunk = m >= kb && m < ke;
-    if (tc2) tma_load_3d(base + L::AUX, &a.mC2, i0, j0, zc + m, bar);
-    if (tdiv && chunk) tma_load_3d(base + L::AUX + L::O_BYTES, &a.mDiv, i0, j0, zc + m, bar);
-    const uint32_t aux = (uint32_t)(((tc2 ? 1 : 0) + (tdiv && chunk ? 1 : 0)) * L::OB * sizeof(T));
+    if (tc2) tma_load_3d(base + L::AUX, &a.mC2, i0 - 4, j0 - 3, zc + m, bar);
+    if (tdiv && chunk) tma_load_3d(base + L::DIV_OFF, &a.mDiv, i0, j0, zc + m, bar);
+    bulk_load(base + L::RAD_OFF, a.radT + (size_t)m * 16, 16 * sizeof(T), bar);
+    const uint32_t aux = (uint32_t)(((tc2 ? L::PB : 0) + (tdiv && chunk ? L::OB : 0) + 16) * sizeof(T));
     if (chunk) {
       const int nbox = has_rho ? 4 : 3;
       mbar_expect_tx(bar, (uint32_t)((2 * nbox * L::PB + 2 * L::OB) * sizeof(T)) + aux);
@@ -173,7 +181,7 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const __grid_cons
   // The 2-D metric terms of the own point and of the halo point are the same on every plane:
   // in float they are held in registers for the whole chunk (the per-plane reads were the
   // kernel's main long-scoreboard stall); in double the 128-register budget has no room and
-  // they are read per plane.
+  // they are read per plane from the interleaved table met8 (four 16-byte loads).
   constexpr bool HOLD = sizeof(T) == 4;
   T gD = T(0), gXYD = T(0), gC = T(0), gXYC = T(0), gDivX = T(0), gDivY = T(0), gTX = T(0), gTY = T(0);
   T gh1 = T(0), gh2 = T(0), gh3 = T(0);
@@ -192,7 +200,8 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const __grid_cons
       gh3 = __ldg(met + (xi_halo ? mDivX : mDivY) * P2 + hq2);
     }
   }
-  auto metric = [&](int row, T held) { return HOLD ? held : __ldg(met + row * P2 + p2); };
+  // in double the eight terms of the own point are read per plane as 16-byte loads
+  const T* met8p = a.met8 + (size_t)p2 * 8;
   int slot = 0;
   uint32_t phase = 0;
   bool ok = true, failed = false;
@@ -202,24 +211,23 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const __grid_cons
     const bool real = (m >= 0 && m < nr);
     const bool own = (m >= kb && m < ke);
     const bool bc = (m == 0 || m == nr - 1);
-    T r1 = T(0), r2 = T(0), part_p = T(0), part_v = T(0);
+    T r1 = T(0), r2 = T(0), part_p = T(0), part_v = T(0), facr_m = T(0);
     if (real) {
       const int o = m * plane + own0;
       const long long plane_c2 = (long long)(face_c2 + m) * P2;
-      // the halo point's c^2 does not come through the ring
       const bool do_halo = own && h_in && !bc;
-      const T hc2 = (do_halo && a.c2) ? __ldg(a.c2 + plane_c2 + hq2) : T(0);
-      const T invr = __ldg(rad + rInvR * nr + m), inv_rho0 = __ldg(rad + rInvRho0 * nr + m);
-      const T rho0 = __ldg(rad + rRho0 * nr + m), c2r = __ldg(rad + rC2Rho0 * nr + m);
       if (ok) {
         ok = mbar_wait(&bars[slot], phase, a.wc, kErrAdjointRing);
         if (ok) m_seen = m + 1;
       }
       const T* sb = reinterpret_cast<const T*>(slot_base(slot));
+      const T* rrow = reinterpret_cast<const T*>(slot_base(slot) + L::RAD_OFF);
+      const T invr = rrow[rInvR], inv_rho0 = rrow[rInvRho0], rho0 = rrow[rRho0], c2r = rrow[rC2Rho0];
+      facr_m = rrow[rFacR];
       constexpr int PBs = (int)(L::P_BYTES / sizeof(T)), OBs = (int)(L::O_BYTES / sizeof(T));
-      const T* saux = reinterpret_cast<const T*>(slot_base(slot) + L::AUX);
-      const T c2own = tc2 ? saux[to] : T(0);
-      const T divv = (own && tdiv) ? saux[OBs + to] : T(0);
+      const T* sc2 = reinterpret_cast<const T*>(slot_base(slot) + L::AUX);
+      const T c2own = tc2 ? sc2[bo] : T(0);
+      const T divv = (own && tdiv) ? sc2[(L::DIV_OFF - L::AUX) / sizeof(T) + to] : T(0);
       T lqv[5], lwv[5];
 #pragma unroll
       for (int f = 0; f < 5; ++f) { lqv[f] = T(0); lwv[f] = T(0); }
@@ -251,12 +259,22 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const __grid_cons
       r1 = -inv_rho0 * mp[kVr];
       r2 = e;
       if (own) {
-        const T tD = metric(mD, gD), tXYD = metric(mXYD, gXYD), tC = metric(mC, gC);
-        const T tXYC = metric(mXYC, gXYC);
+        T mt[8] = {gD, gXYD, gC, gXYC, gDivX, gDivY, gTX, gTY};
+        if (!HOLD) {
+#pragma unroll
+          for (int q = 0; q < 8; q += Vec16<T>::V) {
+            using VT = typename Vec16<T>::type;
+            const VT v = __ldg(reinterpret_cast<const VT*>(met8p + q));
+            const T* e8 = reinterpret_cast<const T*>(&v);
+#pragma unroll
+            for (int u = 0; u < Vec16<T>::V; ++u) mt[q + u] = e8[u];
+          }
+        }
+        const T tD = mt[mD], tXYD = mt[mXYD], tC = mt[mC], tXYC = mt[mXYC];
         sX1[ty][tx + 3] = -invr * inv_rho0 * (tD * mp[kVxi] + tXYC * mp[kVeta]);
-        sX2[ty][tx + 3] = invr * metric(mDivX, gDivX) * e;
+        sX2[ty][tx + 3] = invr * mt[mDivX] * e;
         sY1[ty + 3][tx] = -invr * inv_rho0 * (tXYD * mp[kVxi] + tC * mp[kVeta]);
-        sY2[ty + 3][tx] = invr * metric(mDivY, gDivY) * e;
+        sY2[ty + 3][tx] = invr * mt[mDivY] * e;
         if (has_halo) {
           T v1 = T(0), v2 = T(0);
           if (do_halo) {
@@ -265,7 +283,7 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const __grid_cons
             const T hy = sb[3 * PBs + hb] + a.beta * sb[2 * PBs + hb];
             const T hp = sb[5 * PBs + hb] + a.beta * sb[4 * PBs + hb];
             const T hr = has_rho ? sb[7 * PBs + hb] + a.beta * sb[6 * PBs + hb] : T(0);
-            const T he = -(a.c2 ? hc2 * rho0 : c2r) * hp - rho0 * hr;
+            const T he = -(a.c2 ? sc2[hb] * rho0 : c2r) * hp - rho0 * hr;
             const T hm1 = HOLD ? gh1 : __ldg(met + (xi_halo ? mD : mXYD) * P2 + hq2);
             const T hm2 = HOLD ? gh2 : __ldg(met + (xi_halo ? mXYC : mC) * P2 + hq2);
             const T hm3 = HOLD ? gh3 : __ldg(met + (xi_halo ? mDivX : mDivY) * P2 + hq2);
@@ -276,13 +294,12 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const __grid_cons
           else { sY1[hj + 3][hi] = v1; sY2[hj + 3][hi] = v2; }
         }
         // pointwise terms, lw update, gradient
-        const T sig = __ldg(rad + rSigma * nr + m);
+        const T sig = rrow[rSigma];
         T pw[5];
-        pw[kRho] = -__ldg(rad + rG0Rho0 * nr + m) * mp[kVr] - sig * mu[kRho];
-        pw[kVxi] = -invr * metric(mTX, gTX) * e;
-        pw[kVeta] = -invr * metric(mTY, gTY) * e;
-        pw[kVr] = T(2) * invr * e - __ldg(rad + rDRho0 * nr + m) * mp[kRho] + __ldg(rad + rRho0G0 * nr + m) * mp[kP] -
-                  sig * mu[kVr];
+        pw[kRho] = -rrow[rG0Rho0] * mp[kVr] - sig * mu[kRho];
+        pw[kVxi] = -invr * mt[mTX] * e;
+        pw[kVeta] = -invr * mt[mTY] * e;
+        pw[kVr] = T(2) * invr * e - rrow[rDRho0] * mp[kRho] + rrow[rRho0G0] * mp[kP] - sig * mu[kVr];
         pw[kP] = -sig * mu[kP];
 #pragma unroll
         for (int f = 0; f < 5; ++f) {
@@ -345,7 +362,7 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const __grid_cons
     }
     // radial windows and the partial-output ring advance one plane
     const bool band = real && m >= 3 && m <= nr - 4;
-    const T facr = band ? __ldg(rad + rFacR * nr + m) : T(0);
+    const T facr = band ? facr_m : T(0);
 #pragma unroll
     for (int q = 0; q < 6; ++q) { w1[q] = w1[q + 1]; w2[q] = w2[q + 1]; }
     w1[6] = facr * r1;

@@ -75,6 +75,8 @@ static AdjStageArgs<T> adj_args(solar_ctx* c, double dt) {
   a.grad = nullptr;
   a.rad = (const T*)c->dt.rad;
   a.met = (const T*)c->dt.met;
+  a.radT = (const T*)c->dt.radT;
+  a.met8 = (const T*)c->dt.met8;
   a.g = c->g;
   a.alpha = T(0);
   a.beta = T(1);
@@ -98,7 +100,7 @@ static int launch_adj_stage(solar_ctx* c, AdjStageArgs<T>& a) {
   AdjBuffers& b = c->adj;
   if (!make_map(c, b.L, TX + 8, TY + 6, &a.mBq) || !make_map(c, b.LW, TX + 8, TY + 6, &a.mBw) ||
       !make_map(c, b.L, TX, TY, &a.mTq) || !make_map(c, b.LW, TX, TY, &a.mTw) ||
-      (a.c2 && !make_compact_map(c, a.c2, TX, TY, &a.mC2)) || (a.grad && !make_compact_map(c, a.div, TX, TY, &a.mDiv)))
+      (a.c2 && !make_compact_map(c, a.c2, TX + 8, TY + 6, &a.mC2)) || (a.grad && !make_compact_map(c, a.div, TX, TY, &a.mDiv)))
     return fail(SOLAR_ERR_CUDA, "cuTensorMapEncodeTiled failed");
   if (!a.c2) a.mC2 = a.mTq;                       // unused
   if (!a.grad) a.mDiv = a.mTq;

@@ -111,6 +111,15 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
       : "memory");
 }
 
+// Untiled bulk copy global -> shared of `bytes` bytes (both addresses 16-byte aligned,
+// bytes a multiple of 16), completion signalled on `bar` (transaction bytes).
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
 // Programmatic dependent launch.  A kernel launched with programmatic stream serialization
 // starts as its predecessor's last CTAs exit, before that grid has fully completed; it must
 // call grid_dependency_wait() before it reads anything the predecessor (or an earlier
