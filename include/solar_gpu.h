@@ -248,6 +248,16 @@ int solar_gpu_edge_routes(int* routes);
  * between which a process owning a radial slab receives its neighbours' boundary planes. */
 int solar_gpu_step_phase(solar_ctx* c, int phase);
 
+/* Stage phase p (0..4) in two parts, so that the edge-line exchange of the phase can be in
+ * transit while part 0 runs; the reference overlaps its halo messages with the interior
+ * the same way (derivative.f90:135-148).  Part 0: the stage kernel on the interior tiles,
+ * which read no ghost frame and no line of another zone.  Part 1: the edge kernel, then the
+ * stage kernel on the tiles along the face edges.  Issue part 0 before part 1, with the
+ * phase's radial boundary planes already in place; unpack the received lines between the
+ * two.  Parts 0 and 1 together equal solar_gpu_step_phase(c, p) bit for bit.  A face of
+ * fewer than 3 x 3 stage tiles has no interior: part 0 then launches nothing. */
+int solar_gpu_step_phase_part(solar_ctx* c, int phase, int part);
+
 /* ---- Radial slabs (the reference's pr decomposition, header:6; nruns == 1) -------------
  * The step kernels compute planes k0 .. k1-1 only (k1 - k0 >= 5; default 0 .. nr-1).  The
  * radial stencils near a slab boundary read the neighbouring slab's planes, which the host

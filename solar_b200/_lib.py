@@ -91,6 +91,7 @@ EXPORTS = {
     "solar_gpu_set_owned_zones": [_P, ctypes.c_int, ctypes.c_int],
     "solar_gpu_edge_routes": [_I],
     "solar_gpu_step_phase": [_P, ctypes.c_int],
+    "solar_gpu_step_phase_part": [_P, ctypes.c_int, ctypes.c_int],
     "solar_gpu_set_owned_planes": [_P, ctypes.c_int, ctypes.c_int],
     "solar_gpu_planes_size": [_P, ctypes.c_int],
     "solar_gpu_pack_planes": [_P, ctypes.c_int, ctypes.c_int, ctypes.c_void_p],

@@ -455,7 +455,40 @@ struct StageArgs {
   Geom g;
   T dt, alpha, beta, inv_dxi;
   int kchunk;
+  int tsel;                 // tiles launched: kTilesAll, kTilesInterior or kTilesRing
 };
+
+// Tile subsets of a face (stage_tile).  The interior tiles (1..tx-2) x (1..ty-2) read no
+// ghost frame: their xi and eta halos lie inside the face.  The ring is the tiles along the
+// four face edges.  A process that owns part of the sphere runs the interior tiles while
+// the edge lines of the phase are still in transit, then the ring after the edge kernel.
+enum TileSel { kTilesAll = 0, kTilesInterior = 1, kTilesRing = 2 };
+
+// Tile (ix, iy) of launch index t among tx x ty tiles.  Interior and ring need tx, ty >= 3;
+// the ring lists rows 0 and ty-1, then columns 0 and tx-1 of rows 1..ty-2.
+__host__ __device__ inline void stage_tile(int tsel, int t, int tx, int ty, int* ix, int* iy) {
+  if (tsel == kTilesInterior) {
+    *ix = 1 + t % (tx - 2);
+    *iy = 1 + t / (tx - 2);
+  } else if (tsel == kTilesRing) {
+    if (t < 2 * tx) {
+      *ix = t % tx;
+      *iy = t < tx ? 0 : ty - 1;
+    } else {
+      const int r = t - 2 * tx;
+      *iy = 1 + r / 2;
+      *ix = (r & 1) ? tx - 1 : 0;
+    }
+  } else {
+    *ix = t % tx;
+    *iy = t / tx;
+  }
+}
+__host__ __device__ inline int stage_tile_count(int tsel, int tx, int ty) {
+  if (tsel == kTilesInterior) return (tx - 2) * (ty - 2);
+  if (tsel == kTilesRing) return 2 * tx + 2 * (ty - 2);
+  return tx * ty;
+}
 
 template <typename T, int TX, int TY, bool HAS_RHO>
 struct StageLayout {
@@ -491,7 +524,9 @@ __global__ void __launch_bounds__((TX / Vec16<T>::V) * TY) stage_kernel(const __
   const Geom& g = a.g;
   const int n = g.n, nr = g.nr;
   const int tiles_x = n / TX;
-  const int i0 = (blockIdx.x % tiles_x) * TX, j0 = (blockIdx.x / tiles_x) * TY;
+  int tix, tiy;
+  stage_tile(a.tsel, blockIdx.x, tiles_x, n / TY, &tix, &tiy);
+  const int i0 = tix * TX, j0 = tiy * TY;
   // the run map is written before the launches that use it and constant during them
   const int zr = blockIdx.z / g.nface;
   const int run = a.runs ? a.runs[zr] : zr, face = g.face0 + blockIdx.z % g.nface;

@@ -360,7 +360,9 @@ static int launch_stage_t(solar_ctx* c, StageArgs<T>& a, const void* qin) {
     attr_set = true;
   }
   const int nchunks = (c->g.k1 - c->g.k0 + a.kchunk - 1) / a.kchunk;
-  dim3 grid((c->g.n / TX) * (c->g.n / TY), nchunks, launched_runs(c, a.runs) * c->g.nface);
+  const int ntiles = stage_tile_count(a.tsel, c->g.n / TX, c->g.n / TY);
+  if (ntiles <= 0) return SOLAR_OK;                // no interior tiles at this size
+  dim3 grid(ntiles, nchunks, launched_runs(c, a.runs) * c->g.nface);
   CK(launch_pdl(stage_kernel<T, TX, TY, MODE, HAS_RHO, FORCE>, grid, dim3(TX / Vec16<T>::V, TY), L::TOTAL, c->stream, a));
   return SOLAR_OK;
 }
@@ -400,7 +402,7 @@ static void default_tile(int n, bool fp32, int* tx, int* ty) {
 
 template <typename T>
 static int launch_stage(solar_ctx* c, const void* qin, void* qout, int mode, int stage,
-                        const int* runs, void* divout = nullptr) {
+                        const int* runs, void* divout = nullptr, int tsel = kTilesAll) {
   StageArgs<T> a;
   a.divout = (T*)divout;
   const bool forced = c->forcing && mode != 3;     // every mode but the gradient/divergence operator
@@ -421,6 +423,10 @@ static int launch_stage(solar_ctx* c, const void* qin, void* qout, int mode, int
   a.kchunk = c->kchunk;
   int tx = c->tile_x, ty = c->tile_y;
   if (mode == 2 || mode == 3) default_tile(c->g.n, c->fp32, &tx, &ty);   // operator-level calls
+  // a face of fewer than 3 x 3 tiles has no interior tile: its ring is every tile
+  const bool subsets = c->g.n / tx >= 3 && c->g.n / ty >= 3;
+  a.tsel = subsets ? tsel : (tsel == kTilesInterior ? -1 : kTilesAll);
+  if (a.tsel < 0) return SOLAR_OK;
   if (tx == 16 && ty == 16) return launch_stage_mode<T, 16, 16>(c, a, qin, mode);
   if (tx == 32 && ty == 8) return launch_stage_mode<T, 32, 8>(c, a, qin, mode);
   if (tx == 32 && ty == 16) return launch_stage_mode<T, 32, 16>(c, a, qin, mode);

@@ -74,6 +74,26 @@ static int enqueue_phase(solar_ctx* c, int phase) {
   return force_end(c);
 }
 
+// Phases 0..4 in two parts, so that a process can overlap the edge-line exchange with
+// computation.  Part 0: the stage on the interior tiles, which read no ghost frame and no
+// line of another zone (phase 0 also starts the step's forcing).  Part 1: the edge kernel,
+// then the stage on the ring of face-edge tiles.  Part 0 precedes part 1; the radial slab's
+// boundary planes of the phase must be in place before part 0, the received edge lines
+// before part 1.  The two parts write disjoint points, so together they equal the phase.
+template <typename T>
+static int enqueue_phase_part(solar_ctx* c, int phase, int part) {
+  int rc;
+  void* in = phase % 2 ? c->B : c->A;
+  void* out = phase % 2 ? c->A : c->B;
+  const int mode = phase == 0 ? 1 : 0;
+  if (part == 0) {
+    if (phase == 0 && (rc = force_begin(c))) return rc;
+    return launch_stage<T>(c, in, out, mode, phase, nullptr, nullptr, kTilesInterior);
+  }
+  if ((rc = launch_edge<T>(c, in, 0, nullptr))) return rc;
+  return launch_stage<T>(c, in, out, mode, phase, nullptr, nullptr, kTilesRing);
+}
+
 // Boundary planes exchanged between radial slabs: before stage s the three planes of p and
 // v_r next to each slab boundary (the 7-point radial windows), before FILTER_EXP the five
 // planes of every stored field (the 11-point radial filter; sent after the edge exchange,
@@ -152,6 +172,17 @@ int solar_gpu_step_phase(solar_ctx* c, int phase) {
   if (rc) return rc;
   CK(cudaGetLastError());
   return (phase == 5 || phase == 7) ? watch_after_step(c) : SOLAR_OK;
+}
+
+int solar_gpu_step_phase_part(solar_ctx* c, int phase, int part) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (phase < 0 || phase > 4) return fail(SOLAR_ERR_ARG, "phase parts exist for the stages 0..4 only");
+  if (part < 0 || part > 1) return fail(SOLAR_ERR_ARG, "part must be 0 (interior tiles) or 1 (edge kernel, ring tiles)");
+  rc = c->fp32 ? enqueue_phase_part<float>(c, phase, part) : enqueue_phase_part<double>(c, phase, part);
+  if (rc) return rc;
+  CK(cudaGetLastError());
+  return SOLAR_OK;
 }
 
 int solar_gpu_set_owned_planes(solar_ctx* c, int k0, int k1) {

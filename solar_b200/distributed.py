@@ -148,6 +148,27 @@ class LineExchange:
         self.transport(*self.buffers(phase))
         self.unpack(phase)
 
+    def start(self, phase: int):
+        """Pack this phase's lines and start their transfer without waiting for it; returns
+        the pending transfer for finish().  A transport without ``start``/``finish``
+        attributes moves the lines here, at once."""
+        if self.empty:
+            return None
+        self.pack(phase)
+        begin = getattr(self.transport, "start", None)
+        if begin is None:
+            self.transport(*self.buffers(phase))
+            return None
+        return begin(*self.buffers(phase))
+
+    def finish(self, phase: int, pending) -> None:
+        """Wait for the transfer start() began, then unpack the received lines."""
+        if self.empty:
+            return
+        if pending is not None:
+            self.transport.finish(pending)
+        self.unpack(phase)
+
 
 class _LibPacker:
     """pack/unpack through the C-ABI into CUDA tensors, on the context's stream."""
@@ -237,13 +258,25 @@ class _LibPlanePacker:
         _lib.check(self.s.lib.solar_gpu_unpack_planes(self.s._h, phase, side, ctypes.c_void_p(buf.data_ptr())))
 
 
-def step_sequence(lines: "LineExchange", planes: "PlaneExchange", step_phase) -> None:
+def step_sequence(lines: "LineExchange", planes: "PlaneExchange", step_phase, step_part=None) -> None:
     """One RK4 call of a rank: edge lines and boundary planes before each stage; the filter
-    phase split around its edge exchange, with the filter's boundary planes in between."""
+    phase split around its edge exchange, with the filter's boundary planes in between.
+
+    With ``step_part(phase, part)`` (solar_gpu_step_phase_part) each stage overlaps its line
+    transfer: the boundary planes move first, then the lines are packed and sent, the stage
+    runs on the interior tiles (part 0, which needs no line) while they are in transit, and
+    after they are unpacked the edge kernel and the face-edge tiles run (part 1)."""
     for phase in range(5):
-        lines.run(phase)
+        if step_part is None:
+            lines.run(phase)
+            planes.run(phase)
+            step_phase(phase)
+            continue
         planes.run(phase)
-        step_phase(phase)
+        pending = lines.start(phase)
+        step_part(phase, 0)
+        lines.finish(phase, pending)
+        step_part(phase, 1)
     lines.run(5)
     if planes.empty:
         step_phase(5)
@@ -262,13 +295,25 @@ def p2p_transport(stream=None, group=None):
     import torch
     import torch.distributed as dist
 
-    def run(sends, recvs):
-        ctx = torch.cuda.stream(stream) if stream is not None else contextlib.nullcontext()
-        with ctx:
+    def ctx():
+        return torch.cuda.stream(stream) if stream is not None else contextlib.nullcontext()
+
+    def start(sends, recvs):
+        """Issue the sends and receives; NCCL runs them on its own stream after the packing."""
+        with ctx():
             ops = [dist.P2POp(dist.isend, b, p, group) for p, b in sorted(sends.items())]
             ops += [dist.P2POp(dist.irecv, b, p, group) for p, b in sorted(recvs.items())]
-            for req in dist.batch_isend_irecv(ops):
+            return dist.batch_isend_irecv(ops) if ops else []
+
+    def finish(reqs):
+        """Order ``stream`` after the transfers (NCCL: a stream wait, not a host wait)."""
+        with ctx():
+            for req in reqs:
                 req.wait()
+
+    def run(sends, recvs):
+        finish(start(sends, recvs))
+    run.start, run.finish = start, finish
     return run
 
 
@@ -278,12 +323,14 @@ class ZoneSplitSolver:
     process's GPU, and exchanges edge lines and boundary planes with the other ranks every
     phase.  ``torch.distributed`` must be initialised (NCCL)."""
 
-    def __init__(self, cfg, precision: str = "fp64", nfields: int = 5, device: int = 0, group=None, **kw):
+    def __init__(self, cfg, precision: str = "fp64", nfields: int = 5, device: int = 0, group=None,
+                 overlap: bool = True, **kw):
         import torch
         import torch.distributed as dist
 
         from .solver import Solver
 
+        self.overlap = overlap               # stage interiors run while the lines are in transit
         self.world = dist.get_world_size(group)
         self.rank = dist.get_rank(group)
         self.group = group
@@ -311,8 +358,9 @@ class ZoneSplitSolver:
     def rk4(self, nsteps: int = 1) -> None:
         s = self.solver
         step = lambda phase: _lib.check(s.lib.solar_gpu_step_phase(s._h, phase))
+        part = lambda phase, p: _lib.check(s.lib.solar_gpu_step_phase_part(s._h, phase, p))
         for _ in range(int(nsteps)):
-            step_sequence(self.exchange, self.planes, step)
+            step_sequence(self.exchange, self.planes, step, part if self.overlap else None)
         s.synchronize()
 
     def norm(self, field: int = 4) -> float:

@@ -87,6 +87,7 @@ def test_new_entry_points_reject_a_null_context(lib):
     assert lib.solar_gpu_rk4_norms(None, 0, 4, 2, p) == -5
     assert lib.solar_gpu_set_watchdog(None, 1) == -5
     assert lib.solar_gpu_inject_wait_timeout(None, 1, 100) == -5
+    assert lib.solar_gpu_step_phase_part(None, 0, 0) == -5
 
 
 def test_norm_noalloc_rejects_planes_beyond_int_range_before_any_launch(lib):

@@ -89,8 +89,10 @@ def test_split_run_equals_single_context(cfg, world, precision, nfields):
     assert abs(norm - want_norm) <= 1e-12 * want_norm
 
 
-def emulate_slabs(cfg, world, nsteps, q0, precision, nfields):
-    """World ranks laid out as D.layout(world) zone groups x radial slabs, one context each."""
+def emulate_slabs(cfg, world, nsteps, q0, precision, nfields, parts=False, tile=None):
+    """World ranks laid out as D.layout(world) zone groups x radial slabs, one context each.
+    With ``parts`` every stage runs as solar_gpu_step_phase_part: part 0 (interior tiles) on
+    every rank before any line of the phase is delivered, part 1 after."""
     import ctypes
 
     import torch
@@ -103,7 +105,7 @@ def emulate_slabs(cfg, world, nsteps, q0, precision, nfields):
             zg, sl = divmod(r, nsl)
             z0, nz = D.partition(ngroups)[zg]
             k0, k1 = D.slabs(cfg.nr, nsl)[sl]
-            s = Solver(cfg, precision=precision, nfields=nfields)
+            s = Solver(cfg, precision=precision, nfields=nfields, tile=tile)
             s.set_state(q0)
             _lib.check(s.lib.solar_gpu_set_owned_zones(s._h, z0, nz))
             _lib.check(s.lib.solar_gpu_set_owned_planes(s._h, k0, k1))
@@ -112,9 +114,11 @@ def emulate_slabs(cfg, world, nsteps, q0, precision, nfields):
             px = D.PlaneExchange(below, above, D._LibPlanePacker(s), None, alloc)
             ranks.append((s, lx, px, (z0, nz, k0, k1)))
 
-        def lines(phase):
+        def lines(phase, between=None):
             for s, lx, _, _ in ranks:
                 lx.pack(phase)
+            if between is not None:
+                between()
             for s, _, _, _ in ranks:
                 s.synchronize()
             for r, (_, lx, _, _) in enumerate(ranks):
@@ -141,8 +145,17 @@ def emulate_slabs(cfg, world, nsteps, q0, precision, nfields):
             for s, _, _, _ in ranks:
                 _lib.check(s.lib.solar_gpu_step_phase(s._h, phase))
 
+        def part(phase, p):
+            for s, _, _, _ in ranks:
+                _lib.check(s.lib.solar_gpu_step_phase_part(s._h, phase, p))
+
         for _ in range(nsteps):
             for phase in range(5):
+                if parts:
+                    planes(phase)
+                    lines(phase, between=lambda: part(phase, 0))
+                    part(phase, 1)
+                    continue
                 lines(phase)
                 planes(phase)
                 step(phase)
@@ -177,6 +190,54 @@ def test_zone_and_slab_split_equals_single_context(cfg, world, precision, nfield
     np.testing.assert_array_equal(got, want)
     norm = (sumsq / (cfg.nx * cfg.nx * cfg.nr) * 6.0) ** 0.5
     assert abs(norm - want_norm) <= 1e-12 * want_norm
+
+
+@pytest.fixture(scope="module")
+def cfg64():
+    return configs.c2(nx=64, nr=32, nsteps=3)
+
+
+TILE16 = (16, 16, 0)          # 4 x 4 stage tiles per face: 4 interior, 12 along the edges
+
+
+@pytest.mark.parametrize("tile", [TILE16, None], ids=["16x16", "default"])
+@pytest.mark.parametrize("precision,nfields", [("fp64", 5), ("fp32", 4)])
+def test_phase_parts_equal_rk4(cfg64, tile, precision, nfields):
+    """Parts 0 and 1 of each stage (interior tiles, then edge kernel + edge tiles) give the
+    RK4 step bit for bit; with the default 64 x 8 tile a 64^2 face has no interior tile."""
+    q0 = initial_state(cfg64)
+    with Solver(cfg64, precision=precision, nfields=nfields, tile=tile) as a, \
+            Solver(cfg64, precision=precision, nfields=nfields, tile=tile) as b:
+        a.set_state(q0)
+        b.set_state(q0)
+        a.rk4(2)
+        for _ in range(2):
+            for phase in range(5):
+                _lib.check(b.lib.solar_gpu_step_phase_part(b._h, phase, 0))
+                _lib.check(b.lib.solar_gpu_step_phase_part(b._h, phase, 1))
+            _lib.check(b.lib.solar_gpu_step_phase(b._h, 5))
+        b.synchronize()
+        np.testing.assert_array_equal(a.get_state(), b.get_state())
+
+
+@pytest.mark.parametrize("world", [2, 4])
+@pytest.mark.parametrize("precision,nfields", [("fp64", 5), ("fp32", 4)])
+def test_overlapped_split_equals_single_context(cfg64, world, precision, nfields):
+    """Every rank runs its interior tiles before the phase's lines are delivered."""
+    q0 = initial_state(cfg64)
+    with Solver(cfg64, precision=precision, nfields=nfields, tile=TILE16) as s:
+        s.set_state(q0)
+        s.rk4(3)
+        want = s.get_state()
+    got, _ = emulate_slabs(cfg64, world, 3, q0, precision, nfields, parts=True, tile=TILE16)
+    np.testing.assert_array_equal(got, want)
+
+
+def test_phase_part_arguments(cfg):
+    with Solver(cfg) as s:
+        assert s.lib.solar_gpu_step_phase_part(s._h, 5, 0) == _lib.SOLAR_ERR_ARG     # the filter phase
+        assert s.lib.solar_gpu_step_phase_part(s._h, 0, 2) == _lib.SOLAR_ERR_ARG
+        assert s.lib.solar_gpu_step_phase_part(s._h, -1, 0) == _lib.SOLAR_ERR_ARG
 
 
 def test_plane_exchange_arguments(cfg):

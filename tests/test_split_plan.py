@@ -255,3 +255,78 @@ def test_zone_and_slab_exchange_over_gloo(world):
     for p in procs:
         p.join(timeout=60)
     assert res == {r: 0 for r in range(world)}
+
+
+def _overlap_rank_main(rank, world, port, out):
+    """One RK4 call through D.step_sequence with phase parts: each stage's lines are
+    started, part 0 runs, and by part 1 the lines of the phase must have arrived."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        ngroups, nsl = D.layout(world)
+        zg, sl = divmod(rank, nsl)
+        plan, below, above = D.slab_plan(world, rank)
+        own = D.owners(D.partition(ngroups))
+        own_rank = [D.rank_of(g, sl, nsl) for g in own]
+        lines = _FakePacker(own_rank, rank)
+        planes = _FakePlanePacker(rank)
+        alloc = lambda n: torch.zeros(n, dtype=torch.float64)
+        lx = D.LineExchange(plan, lines, D.p2p_transport(None), alloc)
+        px = D.PlaneExchange(below, above, planes, D.p2p_transport(None), alloc)
+        routes = D.route_table()
+        events = []
+        bad = 0
+
+        def lines_bad(phase):
+            ns = 3 if phase < 5 else 5
+            n = 0
+            for z in range(6):
+                if own_rank[z] != rank:
+                    continue
+                for e in range(4):
+                    pair = (int(routes[z, e, 0]), int(routes[z, e, 1]))
+                    n += not np.array_equal(lines.store[pair], _code(pair, phase, ns))
+            return n
+
+        def step(phase):                     # the filter phase: its lines came before it
+            nonlocal bad
+            events.append(("phase", phase))
+            if phase in (5, 6):
+                bad += lines_bad(5)
+
+        def part(phase, p):
+            nonlocal bad
+            events.append(("part", phase, p))
+            if p == 1:
+                bad += lines_bad(phase)
+                lines.fill(phase + 1)        # the owned lines that the next phase sends
+        lines.fill(0)
+        D.step_sequence(lx, px, step, part)
+        tail = [("phase", 5)] if px.empty else [("phase", 6), ("phase", 7)]
+        bad += events != [("part", ph, p) for ph in range(5) for p in (0, 1)] + tail
+        for phase in range(6):
+            for side, peer in ((0, below), (1, above)):
+                if peer is not None:
+                    bad += not np.all(planes.got[(phase, side)] == float(peer * 100 + (1 - side) * 10 + phase))
+        out.put((rank, int(bad)))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 4, 8])
+def test_overlapped_step_sequence_over_gloo(world):
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_overlap_rank_main, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=180) for _ in range(world))
+    for p in procs:
+        p.join(timeout=60)
+    assert res == {r: 0 for r in range(world)}
