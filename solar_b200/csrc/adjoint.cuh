@@ -216,6 +216,9 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const __grid_cons
       const int o = m * plane + own0;
       const long long plane_c2 = (long long)(face_c2 + m) * P2;
       const bool do_halo = own && h_in && !bc;
+      // the gradient accumulator is read before the ring wait, so that its DRAM latency
+      // passes during the wait and the plane's arithmetic instead of stalling the store
+      const double gacc = (own && a.grad) ? a.grad[plane_c2 + p2] : 0.0;
       if (ok) {
         ok = mbar_wait(&bars[slot], phase, a.wc, kErrAdjointRing);
         if (ok) m_seen = m + 1;
@@ -314,7 +317,7 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const __grid_cons
         }
         if (a.grad) {
           const T c = sqrt(c2rho0 * inv_rho0);
-          a.grad[plane_c2 + p2] += (double)(a.dt * (T(-2) * c * rho0 * divv) * mp[kP]);
+          a.grad[plane_c2 + p2] = gacc + (double)(a.dt * (T(-2) * c * rho0 * divv) * mp[kP]);
         }
         if (m == 1 || m == 2 || m == nr - 3 || m == nr - 2) {
           const int row = m <= 2 ? m - 1 : m - (nr - 3) + 2;
