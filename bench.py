@@ -342,9 +342,10 @@ def e2e_block(cfg, precision: str, nfields: int, args, world: int, local: int):
             "h2d_bytes_per_step": state_bytes / args.steps,
             "d2h_bytes_per_step": (state_bytes + 8 * args.steps) / args.steps,
             "ms_per_step": te * 1e3 / args.steps, "norm_vr_last": float(norms[-1]),
-            "note": "state in from pinned host memory once per job (the stored fields, FP64), K RK4 "
+            "note": "state in from pinned host memory once per job (the stored fields, FP64; an FP32 "
+                    "context rounds them to float on host threads and copies half those bytes), K RK4 "
                     "steps each followed by norm(v_r) (cube.f90:74-78) kept on the device and read "
-                    "back once, state out at the end; host wall clock of the whole job"}
+                    "back once, state out at the end (FP64); host wall clock of the whole job"}
 
 
 def batch_block(device: int):

@@ -1082,6 +1082,15 @@ __global__ void unpack_kernel(const double* __restrict__ src, T* __restrict__ ds
   dst[g.at(k, j, i)] = (T)src[idx];
 }
 
+// FP32 contexts: the compact volume is uploaded as float (rounded on the host).
+__global__ void unpack_f32_kernel(const float* __restrict__ src, float* __restrict__ dst, Geom g) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long V = (long long)g.n * g.n * g.nr;
+  if (idx >= V) return;
+  const int i = idx % g.n, j = (idx / g.n) % g.n, k = idx / ((long long)g.n * g.n);
+  dst[g.at(k, j, i)] = src[idx];
+}
+
 template <typename T>
 __global__ void pack_kernel(const T* __restrict__ src, double* __restrict__ dst, Geom g) {
   const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;

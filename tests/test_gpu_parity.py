@@ -64,6 +64,27 @@ def test_state_roundtrip_fp64(oracle_mod, c1_small):
         assert np.array_equal(s.get_state(), q)
 
 
+@pytest.mark.parametrize("nfields", [4, 5])
+def test_state_roundtrip_fp32(c1_small, nfields):
+    """An FP32 context stores the FP64 state rounded to nearest float (rounded by host
+    threads before the copy, as the device would round it); reading it back is exact.  Values span normal, large, subnormal
+    and underflowing magnitudes; with 4 fields rho is not stored and reads back as zero."""
+    rng = np.random.default_rng(5)
+    with Solver(c1_small, precision="fp32", nfields=nfields) as s:
+        q = random_state(s.state_shape, 2)
+        flat = q.reshape(-1)
+        flat[:64] = rng.standard_normal(64) * 1e-42          # float subnormals
+        flat[64:128] = rng.standard_normal(64) * 1e-47       # below the float range
+        flat[128:192] = rng.standard_normal(64) * 1e37
+        want = q.astype(np.float32).astype(np.float64)
+        if nfields == 4:
+            want[:, 0] = 0.0
+        for _ in range(2):                                   # the second call reuses the pinned blocks
+            s.set_state(q)
+            got = s.get_state()
+            assert np.array_equal(got, want)
+
+
 def test_gaussian_ic_matches_oracle(oracle_mod, c1_small):
     o = oracle_mod.Oracle(c1_small)
     with Solver(c1_small) as s:
