@@ -57,7 +57,6 @@ struct AdjStageArgs {
   const T* rad;
   const T* met;
   const T* radT;      // [nr][16]: the radial rows of a plane together (through the ring)
-  const T* met8;      // [n][n][8]: metric rows mD..mTY of a point together
   WaitCtl wc;         // error word and bound of the ring waits
   Geom g;
   T alpha, beta, dt, inv_dxi;
@@ -178,30 +177,20 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const __grid_cons
   for (int q = 0; q < 7; ++q) { w1[q] = T(0); w2[q] = T(0); }
 #pragma unroll
   for (int q = 0; q < 4; ++q) { pp[q] = T(0); pv[q] = T(0); }
-  // The 2-D metric terms of the own point and of the halo point are the same on every plane:
-  // in float they are held in registers for the whole chunk (the per-plane reads were the
-  // kernel's main long-scoreboard stall); in double the 128-register budget has no room and
-  // they are read per plane from the interleaved table met8 (four 16-byte loads).
-  constexpr bool HOLD = sizeof(T) == 4;
-  T gD = T(0), gXYD = T(0), gC = T(0), gXYC = T(0), gDivX = T(0), gDivY = T(0), gTX = T(0), gTY = T(0);
+  // The 2-D metric terms of the own point and of the halo point are the same on every plane
+  // and are held in registers for the whole chunk (the per-plane reads were the kernel's
+  // main long-scoreboard stall).  In double this spills 28 bytes under the 128-register
+  // budget and still ran 1% faster than four 16-byte reads per plane.
+  const T gD = __ldg(met + mD * P2 + p2), gXYD = __ldg(met + mXYD * P2 + p2);
+  const T gC = __ldg(met + mC * P2 + p2), gXYC = __ldg(met + mXYC * P2 + p2);
+  const T gDivX = __ldg(met + mDivX * P2 + p2), gDivY = __ldg(met + mDivY * P2 + p2);
+  const T gTX = __ldg(met + mTX * P2 + p2), gTY = __ldg(met + mTY * P2 + p2);
   T gh1 = T(0), gh2 = T(0), gh3 = T(0);
-  if (HOLD) {
-    gD = __ldg(met + mD * P2 + p2);
-    gXYD = __ldg(met + mXYD * P2 + p2);
-    gC = __ldg(met + mC * P2 + p2);
-    gXYC = __ldg(met + mXYC * P2 + p2);
-    gDivX = __ldg(met + mDivX * P2 + p2);
-    gDivY = __ldg(met + mDivY * P2 + p2);
-    gTX = __ldg(met + mTX * P2 + p2);
-    gTY = __ldg(met + mTY * P2 + p2);
-    if (h_in) {
-      gh1 = __ldg(met + (xi_halo ? mD : mXYD) * P2 + hq2);
-      gh2 = __ldg(met + (xi_halo ? mXYC : mC) * P2 + hq2);
-      gh3 = __ldg(met + (xi_halo ? mDivX : mDivY) * P2 + hq2);
-    }
+  if (h_in) {
+    gh1 = __ldg(met + (xi_halo ? mD : mXYD) * P2 + hq2);
+    gh2 = __ldg(met + (xi_halo ? mXYC : mC) * P2 + hq2);
+    gh3 = __ldg(met + (xi_halo ? mDivX : mDivY) * P2 + hq2);
   }
-  // in double the eight terms of the own point are read per plane as 16-byte loads
-  const T* met8p = a.met8 + (size_t)p2 * 8;
   int slot = 0;
   uint32_t phase = 0;
   bool ok = true, failed = false;
@@ -262,22 +251,10 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const __grid_cons
       r1 = -inv_rho0 * mp[kVr];
       r2 = e;
       if (own) {
-        T mt[8] = {gD, gXYD, gC, gXYC, gDivX, gDivY, gTX, gTY};
-        if (!HOLD) {
-#pragma unroll
-          for (int q = 0; q < 8; q += Vec16<T>::V) {
-            using VT = typename Vec16<T>::type;
-            const VT v = __ldg(reinterpret_cast<const VT*>(met8p + q));
-            const T* e8 = reinterpret_cast<const T*>(&v);
-#pragma unroll
-            for (int u = 0; u < Vec16<T>::V; ++u) mt[q + u] = e8[u];
-          }
-        }
-        const T tD = mt[mD], tXYD = mt[mXYD], tC = mt[mC], tXYC = mt[mXYC];
-        sX1[ty][tx + 3] = -invr * inv_rho0 * (tD * mp[kVxi] + tXYC * mp[kVeta]);
-        sX2[ty][tx + 3] = invr * mt[mDivX] * e;
-        sY1[ty + 3][tx] = -invr * inv_rho0 * (tXYD * mp[kVxi] + tC * mp[kVeta]);
-        sY2[ty + 3][tx] = invr * mt[mDivY] * e;
+        sX1[ty][tx + 3] = -invr * inv_rho0 * (gD * mp[kVxi] + gXYC * mp[kVeta]);
+        sX2[ty][tx + 3] = invr * gDivX * e;
+        sY1[ty + 3][tx] = -invr * inv_rho0 * (gXYD * mp[kVxi] + gC * mp[kVeta]);
+        sY2[ty + 3][tx] = invr * gDivY * e;
         if (has_halo) {
           T v1 = T(0), v2 = T(0);
           if (do_halo) {
@@ -287,11 +264,8 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const __grid_cons
             const T hp = sb[5 * PBs + hb] + a.beta * sb[4 * PBs + hb];
             const T hr = has_rho ? sb[7 * PBs + hb] + a.beta * sb[6 * PBs + hb] : T(0);
             const T he = -(a.c2 ? sc2[hb] * rho0 : c2r) * hp - rho0 * hr;
-            const T hm1 = HOLD ? gh1 : __ldg(met + (xi_halo ? mD : mXYD) * P2 + hq2);
-            const T hm2 = HOLD ? gh2 : __ldg(met + (xi_halo ? mXYC : mC) * P2 + hq2);
-            const T hm3 = HOLD ? gh3 : __ldg(met + (xi_halo ? mDivX : mDivY) * P2 + hq2);
-            v1 = -invr * inv_rho0 * (hm1 * hx + hm2 * hy);
-            v2 = invr * hm3 * he;
+            v1 = -invr * inv_rho0 * (gh1 * hx + gh2 * hy);
+            v2 = invr * gh3 * he;
           }
           if (xi_halo) { sX1[hj][hi + 3] = v1; sX2[hj][hi + 3] = v2; }
           else { sY1[hj + 3][hi] = v1; sY2[hj + 3][hi] = v2; }
@@ -300,8 +274,8 @@ __global__ void __launch_bounds__(TX * TY, 2) adj_stage_kernel(const __grid_cons
         const T sig = rrow[rSigma];
         T pw[5];
         pw[kRho] = -rrow[rG0Rho0] * mp[kVr] - sig * mu[kRho];
-        pw[kVxi] = -invr * mt[mTX] * e;
-        pw[kVeta] = -invr * mt[mTY] * e;
+        pw[kVxi] = -invr * gTX * e;
+        pw[kVeta] = -invr * gTY * e;
         pw[kVr] = T(2) * invr * e - rrow[rDRho0] * mp[kRho] + rrow[rRho0G0] * mp[kP] - sig * mu[kVr];
         pw[kP] = -sig * mu[kP];
 #pragma unroll

@@ -76,7 +76,6 @@ static AdjStageArgs<T> adj_args(solar_ctx* c, double dt) {
   a.rad = (const T*)c->dt.rad;
   a.met = (const T*)c->dt.met;
   a.radT = (const T*)c->dt.radT;
-  a.met8 = (const T*)c->dt.met8;
   a.g = c->g;
   a.alpha = T(0);
   a.beta = T(1);

@@ -119,7 +119,6 @@ struct DevTables {
   void* rad = nullptr;     // T [kNumRadial][nr]
   void* met = nullptr;     // T [kNumMetric][n][n]
   void* radT = nullptr;    // T [nr][16]   radial rows of one plane together (zero padded)
-  void* met8 = nullptr;    // T [n][n][8]  metric rows kMD..kMTY of one point together
   void* conv = nullptr;    // T [3][4][n][n]
   void* ew = nullptr;      // T [6][4][3][9][n]     folded edge weights (scalar)
   void* eg = nullptr;      // T [6][4][3][9][2][n]  folded edge weights (vector)
@@ -231,14 +230,11 @@ static int upload_tables(solar_ctx* c) {
   if ((rc = upload<T>(&c->dt.rad, c->ht.radial))) return rc;
   if ((rc = upload<T>(&c->dt.met, c->ht.metric))) return rc;
   {
-    const int nr = c->ht.nr, n = c->ht.n;
-    std::vector<double> rt((size_t)nr * 16, 0.0), m8((size_t)n * n * 8);
+    const int nr = c->ht.nr;
+    std::vector<double> rt((size_t)nr * 16, 0.0);
     for (int k = 0; k < nr; ++k)
       for (int q = 0; q < kNumRadial; ++q) rt[(size_t)k * 16 + q] = c->ht.radial[(size_t)q * nr + k];
-    for (size_t p = 0; p < (size_t)n * n; ++p)
-      for (int q = 0; q < 8; ++q) m8[p * 8 + q] = c->ht.metric[(size_t)q * n * n + p];
     if ((rc = upload<T>(&c->dt.radT, rt))) return rc;
-    if ((rc = upload<T>(&c->dt.met8, m8))) return rc;
   }
   if ((rc = upload<T>(&c->dt.ew, c->ht.ew))) return rc;
   if ((rc = upload<T>(&c->dt.eg, c->ht.eg))) return rc;
@@ -874,7 +870,7 @@ int solar_gpu_finalize(solar_ctx* c) {
   if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
   drop_batch_graphs(c);
   void* ptrs[] = {c->A, c->B, c->W, c->stage64, c->part, c->red_out, c->run_order,
-                  c->err, c->dt.rad, c->dt.met, c->dt.radT, c->dt.met8, c->dt.ew, c->dt.eg, c->dt.egc, c->dt.s0t, c->dt.ewin, c->dt.c2,
+                  c->err, c->dt.rad, c->dt.met, c->dt.radT, c->dt.ew, c->dt.eg, c->dt.egc, c->dt.s0t, c->dt.ewin, c->dt.c2,
                   c->dt.rad64, c->dt.vol2, c->dt.drw, c->dt.c2_64, c->dt.tanx, c->dt.gr};
   for (void* p : ptrs)
     if (p) cudaFree(p);
