@@ -24,7 +24,7 @@ TABLE = os.path.join(HERE, "tuned_b200.json")
 CACHE = os.environ.get("SOLAR_TUNE_CACHE", os.path.join(os.path.expanduser("~"), ".cache", "solar_b200", "tuned.json"))
 
 TILES = [(32, 16), (32, 8), (64, 8), (16, 16)]
-CHUNK_DIVISORS = [0, 2, 3, 4, 6]          # 0 = library default; else nr / d planes per CTA
+CHUNK_DIVISORS = [0, 2, 3, 4, 5, 6, 8, 12]   # 0 = library default; else nr / d planes per CTA
 
 
 def key(nx: int, nr: int, precision: str, nfields: int, nruns: int, device_name: str) -> str:
