@@ -161,10 +161,15 @@ static int enqueue_filter_adjoint(solar_ctx* c) {
   adj_filter_r_kernel<T><<<blocks_for(6LL * g.nf * g.n * g.n, 128), 128, 0, c->stream>>>(L, T1, g);
   constexpr int KP = 8;                                             // planes per CTA
   const unsigned kch = (unsigned)((g.nr + KP - 1) / KP);
-  if (g.n % 32 == 0)
-    adj_filter_xy_kernel<T, 32, 8, KP><<<dim3((g.n / 32) * (g.n / 8), kch, 6 * g.nf), 256, 0, c->stream>>>(T1, L, g);
-  else
-    adj_filter_xy_kernel<T, 16, 16, KP><<<dim3((g.n / 16) * (g.n / 16), kch, 6 * g.nf), 256, 0, c->stream>>>(T1, L, g);
+  constexpr int V = Vec16<T>::V;
+  if (g.n % 32 == 0) {
+    constexpr int TY = sizeof(T) == 4 ? 16 : 8;
+    adj_filter_xyv_kernel<T, 32, TY><<<dim3((g.n / 32) * (g.n / TY), kch, 6 * g.nf), dim3(32 / V, TY), 0, c->stream>>>(
+        T1, L, g, KP);
+  } else {
+    adj_filter_xyv_kernel<T, 16, 16><<<dim3((g.n / 16) * (g.n / 16), kch, 6 * g.nf), dim3(16 / V, 16), 0, c->stream>>>(
+        T1, L, g, KP);
+  }
   adj_edge_kernel<T><<<dim3(blocks_for(g.n, 128), 72, g.nr), 128, g.nf * g.n * sizeof(T), c->stream>>>(
       L, (const T*)c->adj.wt, c->adj.wt_span, c->adj.tspan, g, 1);
   CK(cudaGetLastError());
